@@ -1,0 +1,515 @@
+// edx_krylov.cu -- Lanczos / Krylov recurrences (K9), shifted MINRES (K12), continued
+// fraction (K13) and density matrix (K14).
+//
+// All recurrences keep their scalars (alpha, beta, Givens rotations) in device memory so
+// that an iteration is a fixed sequence of launches with no host round trip; the host only
+// polls a "columns still active" counter every few iterations to stop launching.  Reductions
+// are deterministic: every block writes per-column partial sums, and the last block to
+// finish (atomic ticket) adds them in block order.
+#include <vector>
+
+#include "edx_fock.cuh"
+#include "edx_spmm.cuh"
+
+namespace edx {
+
+int spmm_dispatch(const edx_csr* A, int k, int vec_type, const void* x, int64_t ldx_, void* y, int64_t ldy,
+                  int64_t ycs, double2 al, double2 sg, double2 be, int kw, cudaStream_t st);
+int check_csr(const edx_csr* A);
+int auto_kw(int k);
+
+constexpr int KT = 256;  // threads per block for the recurrence kernels
+
+// ---- deterministic cross-block reduction --------------------------------------------
+__device__ __forceinline__ bool arrive_last(unsigned* ticket) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned total = gridDim.x * gridDim.y;
+        last = (atomicAdd(ticket, 1u) == total - 1u);
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// Sum a per-thread value over threads of the block that share local column c (there are
+// `groups` of them, laid out as sh[g*KW + c]); result written to part[bx*k + gc].
+template <int KW>
+__device__ __forceinline__ void block_col_partial(double v, bool writer, int g, int groups, int c, int k,
+                                                  double* part) {
+    __shared__ double sh[KT];
+    if (writer) sh[g * KW + c] = v;
+    __syncthreads();
+    if (threadIdx.x < KW) {
+        double s = 0.0;
+        for (int q = 0; q < groups; ++q) s += sh[q * KW + threadIdx.x];
+        const int gcol = blockIdx.y * KW + threadIdx.x;
+        if (gcol < k) part[(int64_t)blockIdx.x * k + gcol] = s;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double sum_partials(const double* part, int nbx, int k, int gc) {
+    double s = 0.0;
+    for (int b = 0; b < nbx; ++b) s += __ldcg(part + (int64_t)b * k + gc);
+    return s;
+}
+
+struct KrylovState {
+    double* alpha_out;  // [k*maxn]
+    double* beta_out;   // [k*maxn]
+    int32_t* neff;      // [k]
+    double* alpha;      // [k] current alpha
+    double* beta;       // [k] current beta (beta_{i} after K_b; beta_{i-1} during K_a)
+    int* active;        // [k]
+    int* n_active;      // [1]
+    double* part;       // [GX*k]
+    unsigned* ticket;   // [4]
+    int maxn, k;
+};
+
+// ---- K9a: W = A V_cur - beta_{i-1} V_prev (into V_prev), alpha partials ---------------
+template <int KW, class VT>
+__global__ void __launch_bounds__(KT) k_lanczos_apply(int64_t n, const int64_t* __restrict__ row_ptr,
+                                                      const int32_t* __restrict__ col, const VT* __restrict__ val,
+                                                      const double2* __restrict__ Vc, double2* __restrict__ Vp,
+                                                      KrylovState S, int it) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c = lane % KW;
+    const int k = S.k;
+    const int gc = blockIdx.y * KW + c;
+    const bool colok = gc < k;
+    const double bprev = (colok && it > 0) ? S.beta[gc] : 0.0;
+    double apart = 0.0;
+    const int64_t warp0 = (int64_t)blockIdx.x * (KT / 32) + warp;
+    const int64_t nw = (int64_t)gridDim.x * (KT / 32);
+    for (int64_t r = warp0; r < n; r += nw) {
+        const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
+        double2 acc = row_times_x<KW, VT, double2>(s, e, col, val, Vc, k, gc, colok);
+        if (lane < KW && colok) {
+            const int64_t o = r * k + gc;
+            double2 vp = Vp[o];
+            double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
+            w.x = w.x + acc.x;
+            w.y = w.y + acc.y;
+            Vp[o] = w;
+            double2 vc = Vc[o];
+            apart += vc.x * w.x + vc.y * w.y;  // Re(conj(v) w)
+        }
+    }
+    block_col_partial<KW>(apart, lane < KW, warp, KT / 32, c, k, S.part);
+    if (arrive_last(S.ticket)) {
+        for (int j = threadIdx.x; j < k; j += KT) {
+            double a = sum_partials(S.part, gridDim.x, k, j);
+            S.alpha[j] = a;
+            if (S.active[j]) S.alpha_out[(int64_t)j * S.maxn + it] = a;
+        }
+        if (threadIdx.x == 0) *S.ticket = 0u;
+    }
+}
+
+// ---- K9b: W -= alpha V_cur, beta = |W| ------------------------------------------------
+template <int KW>
+__global__ void __launch_bounds__(KT) k_lanczos_orth(int64_t n, const double2* __restrict__ Vc,
+                                                     double2* __restrict__ Vp, KrylovState S, int it) {
+    const int k = S.k;
+    const int c = threadIdx.x % KW, g = threadIdx.x / KW, groups = KT / KW;
+    const int gc = blockIdx.y * KW + c;
+    const bool colok = gc < k;
+    const double a = colok ? S.alpha[gc] : 0.0;
+    double part = 0.0;
+    if (colok) {
+        for (int64_t r = (int64_t)blockIdx.x * groups + g; r < n; r += (int64_t)gridDim.x * groups) {
+            const int64_t o = r * k + gc;
+            double2 w = Vp[o], v = Vc[o];
+            w.x = w.x - a * v.x;
+            w.y = w.y - a * v.y;
+            Vp[o] = w;
+            part += w.x * w.x + w.y * w.y;
+        }
+    }
+    block_col_partial<KW>(part, true, g, groups, c, k, S.part);
+    if (arrive_last(S.ticket + 1)) {
+        int cnt = 0;
+        for (int j = threadIdx.x; j < k; j += KT) {
+            double b = sqrt(sum_partials(S.part, gridDim.x, k, j));
+            if (S.active[j]) {
+                S.beta_out[(int64_t)j * S.maxn + it] = b;
+                S.neff[j] = it + 1;
+                if (fabs(b) < 1e-10) S.active[j] = 0;
+            }
+            S.beta[j] = b;
+            cnt += S.active[j];
+        }
+        // count active columns
+        __shared__ int scnt[KT];
+        scnt[threadIdx.x] = cnt;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int q = 0; q < KT; ++q) t += scnt[q];
+            *S.n_active = t;
+            S.ticket[1] = 0u;
+        }
+    }
+}
+
+// ---- K9c: V_next = W / beta (inactive columns -> 0) ------------------------------------
+__global__ void k_lanczos_scale(int64_t n, int k, double2* __restrict__ Vp, const double* __restrict__ beta,
+                                const int* __restrict__ active) {
+    const int64_t total = n * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % k);
+        double2 w = Vp[e];
+        if (active[c]) {
+            const double b = beta[c];
+            w.x = w.x / b;
+            w.y = w.y / b;
+        } else {
+            w.x = 0.0;
+            w.y = 0.0;
+        }
+        Vp[e] = w;
+    }
+}
+
+// ---- start vectors: norm and normalisation --------------------------------------------
+template <int KW>
+__global__ void __launch_bounds__(KT) k_colnorm(int64_t n, const double2* __restrict__ V0, KrylovState S) {
+    const int k = S.k;
+    const int c = threadIdx.x % KW, g = threadIdx.x / KW, groups = KT / KW;
+    const int gc = blockIdx.y * KW + c;
+    double part = 0.0;
+    if (gc < k)
+        for (int64_t r = (int64_t)blockIdx.x * groups + g; r < n; r += (int64_t)gridDim.x * groups) {
+            double2 v = V0[r * k + gc];
+            part += v.x * v.x + v.y * v.y;
+        }
+    block_col_partial<KW>(part, true, g, groups, c, k, S.part);
+    if (arrive_last(S.ticket + 2)) {
+        for (int j = threadIdx.x; j < k; j += KT) {
+            double s = sum_partials(S.part, gridDim.x, k, j);
+            S.alpha[j] = s;  // <v0|v0>, handed to the host-side norm output
+            S.beta[j] = sqrt(s);
+            S.active[j] = 1;
+            S.neff[j] = 0;
+        }
+        if (threadIdx.x == 0) S.ticket[2] = 0u;
+    }
+}
+
+__global__ void k_start(int64_t n, int k, const double2* __restrict__ V0, double2* __restrict__ Vc,
+                        double2* __restrict__ Vp, const double* __restrict__ s) {
+    const int64_t total = n * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e % k);
+        double2 v = V0[e];
+        const double d = s[c];
+        Vc[e] = make_double2(v.x / d, v.y / d);
+        Vp[e] = make_double2(0.0, 0.0);
+    }
+}
+
+// ---- K12: per-shift MINRES recurrences in the Lanczos basis ----------------------------
+struct ShiftState {
+    double2 gamma0, gamma1, sigma0, sigma1, eta;
+    double beta0, res;
+    int frozen, iters;
+};
+
+__global__ void k_shift_init(int nshift, const int32_t* __restrict__ scol, const double* __restrict__ norm2,
+                             ShiftState* __restrict__ st, double tol, int maxit) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nshift) return;
+    const double b0 = sqrt(norm2[scol[s]]);
+    ShiftState q;
+    q.gamma0 = make_double2(1.0, 0.0);
+    q.gamma1 = make_double2(1.0, 0.0);
+    q.sigma0 = make_double2(0.0, 0.0);
+    q.sigma1 = make_double2(0.0, 0.0);
+    q.eta = make_double2(b0, 0.0);
+    q.beta0 = b0;
+    q.res = b0;
+    q.iters = 0;
+    q.frozen = !(fabs(b0) > tol && 0 < maxit);
+    st[s] = q;
+}
+
+// one warp per shift; lanes share the scalar work and split the coefficient vectors
+__global__ void k_shift_step(int nshift, const int32_t* __restrict__ scol, const double2* __restrict__ sz,
+                             ShiftState* __restrict__ st, double2* __restrict__ wbuf, double2* __restrict__ y,
+                             KrylovState S, int it, double tol, int maxit, int* __restrict__ n_open) {
+    const int lane = threadIdx.x & 31;
+    const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (s >= nshift) return;
+    ShiftState q = st[s];
+    if (q.frozen) return;
+    const int c = scol[s];
+    if (S.neff[c] != it + 1) {  // the column's recurrence stopped before this iteration
+        if (lane == 0) {
+            q.frozen = 1;
+            st[s] = q;
+        }
+        return;
+    }
+    const int64_t m = S.maxn;
+    const double a_h = S.alpha_out[(int64_t)c * m + it];
+    const double beta1 = S.beta_out[(int64_t)c * m + it];
+    const double2 z = sz[s];
+    const double2 alpha = make_double2(z.x - a_h, z.y);
+    // linsys.f90:92-101
+    const double2 delta = csub(cmul(q.gamma0, alpha), cscale(cmul(q.gamma1, q.sigma0), q.beta0));
+    const double2 rho1 = csqrt_(cadd(cmul(delta, delta), make_double2(beta1 * beta1, 0.0)));
+    const double2 rho2 = cadd(cmul(q.sigma0, alpha), cscale(cmul(q.gamma1, q.gamma0), q.beta0));
+    const double2 rho3 = cscale(q.sigma1, q.beta0);
+    q.gamma1 = q.gamma0;
+    q.sigma1 = q.sigma0;
+    q.gamma0 = cdiv(delta, rho1);
+    q.sigma0 = cdiv(make_double2(beta1, 0.0), rho1);
+    const double2 ge = cmul(q.gamma0, q.eta);
+    // coefficient vectors: prev slot holds w_{it-2}, curr slot w_{it-1}; v_it = (-1)^it u_it
+    double2* wprev = wbuf + ((int64_t)s * 2 + (it & 1)) * m;
+    const double2* wcurr = wbuf + ((int64_t)s * 2 + ((it + 1) & 1)) * m;
+    double2* ys = y + (int64_t)s * m;
+    const double sgn = (it & 1) ? -1.0 : 1.0;
+    for (int j = lane; j <= it; j += 32) {
+        double2 v = make_double2(j == it ? sgn : 0.0, 0.0);
+        double2 t = csub(csub(v, cmul(rho3, wprev[j])), cmul(rho2, wcurr[j]));
+        double2 wn = cdiv(t, rho1);
+        wprev[j] = wn;
+        ys[j] = cadd(ys[j], cmul(ge, wn));
+    }
+    if (lane == 0) {
+        q.res = cabs_(q.sigma0) * q.res;
+        q.eta = cmul(make_double2(-q.sigma0.x, -q.sigma0.y), q.eta);
+        q.beta0 = beta1;
+        q.iters = it + 1;
+        q.frozen = !(q.res > tol && q.iters < maxit);
+        st[s] = q;
+        if (!q.frozen) atomicAdd(n_open, 1);
+    }
+}
+
+__global__ void k_shift_final(int nshift, const ShiftState* __restrict__ st, int32_t* iters, double* res) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nshift) return;
+    if (iters) iters[s] = st[s].iters;
+    if (res) res[s] = st[s].res;
+}
+
+template <int KW, class VT>
+static int launch_apply(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+                        int gx, cudaStream_t st) {
+    dim3 grid(gx, (S.k + KW - 1) / KW);
+    k_lanczos_apply<KW, VT><<<grid, KT, 0, st>>>(A->nrows, A->row_ptr, A->col,
+                                                 reinterpret_cast<const VT*>(A->val), Vc, Vp, S, it);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}
+
+template <class VT>
+static int apply_v(int kw, const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+                   int gx, cudaStream_t st) {
+    switch (kw) {
+    case 1: return launch_apply<1, VT>(A, Vc, Vp, S, it, gx, st);
+    case 2: return launch_apply<2, VT>(A, Vc, Vp, S, it, gx, st);
+    case 4: return launch_apply<4, VT>(A, Vc, Vp, S, it, gx, st);
+    case 8: return launch_apply<8, VT>(A, Vc, Vp, S, it, gx, st);
+    case 16: return launch_apply<16, VT>(A, Vc, Vp, S, it, gx, st);
+    case 32: return launch_apply<32, VT>(A, Vc, Vp, S, it, gx, st);
+    }
+    return fail(EDX_ERR_INVALID, "krylov: bad column group %d", kw);
+}
+
+#define EDX_KW_SWITCH(kw, KERNEL, GRID, ...)                                                  \
+    switch (kw) {                                                                              \
+    case 1: KERNEL<1><<<GRID, KT, 0, st>>>(__VA_ARGS__); break;                               \
+    case 2: KERNEL<2><<<GRID, KT, 0, st>>>(__VA_ARGS__); break;                               \
+    case 4: KERNEL<4><<<GRID, KT, 0, st>>>(__VA_ARGS__); break;                               \
+    case 8: KERNEL<8><<<GRID, KT, 0, st>>>(__VA_ARGS__); break;                               \
+    case 16: KERNEL<16><<<GRID, KT, 0, st>>>(__VA_ARGS__); break;                             \
+    default: KERNEL<32><<<GRID, KT, 0, st>>>(__VA_ARGS__); break;                             \
+    }
+
+struct KrylovWs {
+    double2 *Vc, *Vp;
+    double *alpha, *beta, *part;
+    int *active, *n_active, *n_open;
+    unsigned* ticket;
+    ShiftState* sst;
+    double2* wbuf;
+};
+
+static int reduce_grid(int64_t n) {
+    int64_t g = (int64_t)num_sms() * 4;
+    int64_t need = (n + 63) / 64;
+    if (need < g) g = need;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <class WS>
+static void krylov_layout(WS& w, int64_t n, int k, int nshift, int maxn, int gx, KrylovWs* out) {
+    auto Vc = w.template take<double2>((size_t)(n * k));
+    auto Vp = w.template take<double2>((size_t)(n * k));
+    auto al = w.template take<double>((size_t)k);
+    auto be = w.template take<double>((size_t)k);
+    auto pa = w.template take<double>((size_t)gx * k);
+    auto ac = w.template take<int>((size_t)k);
+    auto na = w.template take<int>(2);
+    auto tk = w.template take<unsigned>(4);
+    auto ss = w.template take<ShiftState>((size_t)(nshift > 0 ? nshift : 1));
+    auto wb = w.template take<double2>((size_t)(nshift > 0 ? 2 * (size_t)nshift * maxn : 1));
+    if (out) {
+        out->Vc = Vc;
+        out->Vp = Vp;
+        out->alpha = al;
+        out->beta = be;
+        out->part = pa;
+        out->active = ac;
+        out->n_active = na;
+        out->n_open = na + 1;
+        out->ticket = tk;
+        out->sst = ss;
+        out->wbuf = wb;
+    }
+}
+
+// WorkspaceSize::take returns void; wrap it so krylov_layout can use one template
+struct SizeOnly {
+    WorkspaceSize s;
+    template <class T>
+    T* take(size_t c) {
+        s.take<T>(c);
+        return nullptr;
+    }
+};
+
+}  // namespace edx
+
+using namespace edx;
+
+extern "C" int edx_krylov_workspace(int64_t n, int k, const edx_krylov_opts* opts, int maxn, size_t* bytes) {
+    EDX_REQUIRE(bytes != nullptr && n >= 1 && k >= 1 && maxn >= 1, "edx_krylov_workspace: bad arguments");
+    SizeOnly s;
+    int gx = reduce_grid(n);
+    if (gx < num_sms() * 4) gx = num_sms() * 4;  // the apply kernel's grid can be larger
+    krylov_layout(s, n, k, opts ? opts->nshift : 0, maxn, gx, nullptr);
+    *bytes = s.s.bytes();
+    return EDX_OK;
+}
+
+extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn, double* d_alpha, double* d_beta,
+                          double* d_norm, int32_t* d_neff, const edx_krylov_opts* opts, void* d_work,
+                          size_t work_bytes, void* stream) {
+    int rc = check_csr(A);
+    if (rc) return rc;
+    EDX_REQUIRE(A->nrows == A->ncols && A->nrows >= 1, "edx_krylov: matrix must be square and non-empty");
+    EDX_REQUIRE(k >= 1 && maxn >= 1 && d_v0 && d_alpha && d_beta && d_norm && d_neff,
+                "edx_krylov: bad arguments");
+    const int nshift = opts ? opts->nshift : 0;
+    const int nproj = opts ? opts->nproj : 0;
+    if (nshift > 0)
+        EDX_REQUIRE(opts->shift_col && opts->shift_z && opts->shift_y, "edx_krylov: shift arrays missing");
+    for (int p = 0; p < nproj; ++p) {
+        EDX_REQUIRE(opts->proj && opts->proj_out && opts->proj_out[p], "edx_krylov: projection %d missing", p);
+        rc = check_csr(&opts->proj[p]);
+        if (rc) return rc;
+        EDX_REQUIRE(opts->proj[p].ncols == A->nrows, "edx_krylov: projection %d has wrong width", p);
+    }
+    cudaStream_t st = as_stream(stream);
+    const int64_t n = A->nrows;
+    const int kw = auto_kw(k);
+    const int gy = (k + kw - 1) / kw;
+    int gx = num_sms() * 4;
+    Workspace w(d_work, work_bytes);
+    KrylovWs ws;
+    krylov_layout(w, n, k, nshift, maxn, gx, &ws);
+    if (!ws.wbuf) return fail(EDX_ERR_WORKSPACE, "edx_krylov: workspace too small");
+
+    KrylovState S;
+    S.alpha_out = d_alpha;
+    S.beta_out = d_beta;
+    S.neff = d_neff;
+    S.alpha = ws.alpha;
+    S.beta = ws.beta;
+    S.active = ws.active;
+    S.n_active = ws.n_active;
+    S.part = ws.part;
+    S.ticket = ws.ticket;
+    S.maxn = maxn;
+    S.k = k;
+
+    EDX_CUDA(cudaMemsetAsync(ws.ticket, 0, 4 * sizeof(unsigned), st));
+    EDX_CUDA(cudaMemsetAsync(d_alpha, 0, sizeof(double) * (size_t)k * maxn, st));
+    EDX_CUDA(cudaMemsetAsync(d_beta, 0, sizeof(double) * (size_t)k * maxn, st));
+    const double2* V0 = reinterpret_cast<const double2*>(d_v0);
+    {
+        dim3 grid(reduce_grid(n), gy);
+        EDX_KW_SWITCH(kw, k_colnorm, grid, n, V0, S);
+        EDX_CHECK_LAUNCH();
+    }
+    EDX_CUDA(cudaMemcpyAsync(d_norm, ws.alpha, sizeof(double) * k, cudaMemcpyDeviceToDevice, st));
+    const int eb = (int)std::min<int64_t>((n * k + 255) / 256, (int64_t)num_sms() * 16);
+    k_start<<<eb, 256, 0, st>>>(n, k, V0, ws.Vc, ws.Vp, ws.beta);
+    EDX_CHECK_LAUNCH();
+    if (nshift > 0) {
+        EDX_CUDA(cudaMemsetAsync(ws.wbuf, 0, sizeof(double2) * 2 * (size_t)nshift * maxn, st));
+        EDX_CUDA(cudaMemsetAsync(opts->shift_y, 0, sizeof(double2) * (size_t)nshift * maxn, st));
+        k_shift_init<<<(nshift + 127) / 128, 128, 0, st>>>(nshift, opts->shift_col, ws.alpha, ws.sst,
+                                                           opts->shift_tol, opts->shift_maxit);
+        EDX_CHECK_LAUNCH();
+    }
+    auto project = [&](const double2* V, int i) -> int {
+        for (int p = 0; p < nproj; ++p) {
+            const edx_csr* P = &opts->proj[p];
+            double2* out = reinterpret_cast<double2*>(opts->proj_out[p]) + (int64_t)i * P->nrows;
+            int r2 = spmm_dispatch(P, k, EDX_C128, V, k, out, 1, (int64_t)maxn * P->nrows,
+                                   make_double2(1, 0), make_double2(0, 0), make_double2(0, 0), 0, st);
+            if (r2) return r2;
+        }
+        return EDX_OK;
+    };
+    if ((rc = project(ws.Vc, 0))) return rc;
+
+    double2* Vc = ws.Vc;
+    double2* Vp = ws.Vp;
+    const int poll = 8;
+    for (int it = 0; it < maxn; ++it) {
+        if (nshift > 0) EDX_CUDA(cudaMemsetAsync(ws.n_open, 0, sizeof(int), st));
+        rc = (A->val_type == EDX_C128) ? apply_v<double2>(kw, A, Vc, Vp, S, it, gx, st)
+                                       : apply_v<float2>(kw, A, Vc, Vp, S, it, gx, st);
+        if (rc) return rc;
+        {
+            dim3 grid(reduce_grid(n), gy);
+            EDX_KW_SWITCH(kw, k_lanczos_orth, grid, n, Vc, Vp, S, it);
+            EDX_CHECK_LAUNCH();
+        }
+        if (nshift > 0) {
+            k_shift_step<<<(nshift * 32 + 255) / 256, 256, 0, st>>>(
+                nshift, opts->shift_col, reinterpret_cast<const double2*>(opts->shift_z), ws.sst, ws.wbuf,
+                reinterpret_cast<double2*>(opts->shift_y), S, it, opts->shift_tol, opts->shift_maxit, ws.n_open);
+            EDX_CHECK_LAUNCH();
+        }
+        k_lanczos_scale<<<eb, 256, 0, st>>>(n, k, Vp, ws.beta, ws.active);
+        EDX_CHECK_LAUNCH();
+        std::swap(Vc, Vp);
+        if (it + 1 < maxn && (rc = project(Vc, it + 1))) return rc;
+        if ((it + 1) % poll == 0 || it + 1 == maxn) {
+            int h[2] = {0, 0};
+            EDX_CUDA(cudaMemcpyAsync(h, ws.n_active, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            EDX_CUDA(cudaStreamSynchronize(st));
+            if (h[0] == 0) break;
+            if (nshift > 0 && h[1] == 0) break;
+        }
+    }
+    if (nshift > 0) {
+        k_shift_final<<<(nshift + 127) / 128, 128, 0, st>>>(nshift, ws.sst, opts->shift_iters, opts->shift_res);
+        EDX_CHECK_LAUNCH();
+    }
+    return EDX_OK;
+}

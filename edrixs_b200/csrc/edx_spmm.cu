@@ -1,0 +1,133 @@
+// edx_spmm.cu -- complex CSR SpMV / SpMM (kernels K7, K8).
+//
+// Y = alpha*(A X) + sigma*X + beta*Y over k right-hand sides.  matvec_csr
+// (src/spmv.f90:73-103) is the k = 1, alpha = 1, beta = 1, sigma = 0 case (y += A x).  One
+// warp per row; lanes are split into SLOTS = 32/KW slots x KW columns so that a row's
+// nonzeros stream through the warp in coalesced 32-entry chunks (column indices and values
+// each loaded once, with L1 no-allocate / L2 evict-first hints since the matrix is read
+// once per product) while the gathered X rows stay L2-resident.  Column tiles of width KW
+// run as grid.y so that wide blocks (k = 768) keep one X tile hot in L2 at a time.
+#include "edx_spmm.cuh"
+
+namespace edx {
+
+template <int KW, class VT, class XT>
+__global__ void __launch_bounds__(256) k_spmm(int64_t nrows, const int64_t* __restrict__ row_ptr,
+                                              const int32_t* __restrict__ col, const VT* __restrict__ val,
+                                              int k, const XT* __restrict__ X, int64_t ldx_, XT* __restrict__ Y,
+                                              int64_t ldy, int64_t ycs, double2 alpha, double2 sigma,
+                                              double2 beta, int has_sigma, int has_beta) {
+    using AT = typename Acc<VT, XT>::T;
+    const int lane = threadIdx.x & 31;
+    const int c = lane % KW;
+    const int gc = blockIdx.y * KW + c;
+    const bool colok = gc < k;
+    const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = warp0; r < nrows; r += nw) {
+        const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
+        AT acc = row_times_x<KW, VT, XT>(s, e, col, val, X, ldx_, gc, colok);
+        if (lane < KW && colok) {
+            double yr = alpha.x * (double)acc.x - alpha.y * (double)acc.y;
+            double yi = alpha.x * (double)acc.y + alpha.y * (double)acc.x;
+            if (has_sigma) {
+                XT xv = X[r * ldx_ + gc];
+                yr += sigma.x * (double)xv.x - sigma.y * (double)xv.y;
+                yi += sigma.x * (double)xv.y + sigma.y * (double)xv.x;
+            }
+            XT* yp = Y + r * ldy + (int64_t)gc * ycs;
+            if (has_beta) {
+                XT yv = *yp;
+                yr += beta.x * (double)yv.x - beta.y * (double)yv.y;
+                yi += beta.x * (double)yv.y + beta.y * (double)yv.x;
+            }
+            XT out;
+            out.x = yr;
+            out.y = yi;
+            *yp = out;
+        }
+    }
+}
+
+template <int KW, class VT, class XT>
+static int launch_spmm_t(const edx_csr* A, int k, const void* x, int64_t ldx_, void* y, int64_t ldy,
+                         int64_t ycs, double2 al, double2 sg, double2 be, cudaStream_t st) {
+    const int threads = 256;
+    int64_t need = (A->nrows * 32 + threads - 1) / threads;
+    int64_t maxb = (int64_t)num_sms() * 8;
+    int64_t bx = need < maxb ? need : maxb;
+    if (bx < 1) bx = 1;
+    dim3 grid((unsigned)bx, (unsigned)((k + KW - 1) / KW));
+    const int hs = (sg.x != 0.0 || sg.y != 0.0) ? 1 : 0;
+    const int hb = (be.x != 0.0 || be.y != 0.0) ? 1 : 0;
+    k_spmm<KW, VT, XT><<<grid, threads, 0, st>>>(A->nrows, A->row_ptr, A->col,
+                                                  reinterpret_cast<const VT*>(A->val), k,
+                                                  reinterpret_cast<const XT*>(x), ldx_,
+                                                  reinterpret_cast<XT*>(y), ldy, ycs, al, sg, be, hs, hb);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}
+
+template <class VT, class XT>
+static int launch_spmm_v(const edx_csr* A, int k, int kw, const void* x, int64_t ldx_, void* y,
+                         int64_t ldy, int64_t ycs, double2 al, double2 sg, double2 be, cudaStream_t st) {
+    switch (kw) {
+    case 1: return launch_spmm_t<1, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    case 2: return launch_spmm_t<2, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    case 4: return launch_spmm_t<4, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    case 8: return launch_spmm_t<8, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    case 16: return launch_spmm_t<16, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    case 32: return launch_spmm_t<32, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    }
+    return fail(EDX_ERR_INVALID, "spmm: unsupported column group width %d", kw);
+}
+
+int auto_kw(int k) {
+    int kw = 1;
+    while (kw < k && kw < 32) kw <<= 1;
+    return kw;
+}
+
+int check_csr(const edx_csr* A) {
+    EDX_REQUIRE(A != nullptr, "NULL matrix");
+    EDX_REQUIRE(A->nrows >= 0 && A->ncols >= 0 && A->nnz >= 0, "matrix with negative size");
+    EDX_REQUIRE(A->nrows == 0 || A->row_ptr != nullptr, "matrix without row pointers");
+    EDX_REQUIRE(A->nnz == 0 || (A->col != nullptr && A->val != nullptr), "matrix without entries");
+    EDX_REQUIRE(A->val_type == EDX_C128 || A->val_type == EDX_C64, "matrix value type %d", A->val_type);
+    return EDX_OK;
+}
+
+int spmm_dispatch(const edx_csr* A, int k, int vec_type, const void* x, int64_t ldx_, void* y, int64_t ldy,
+                  int64_t ycs, double2 al, double2 sg, double2 be, int kw, cudaStream_t st) {
+    if (kw <= 0) kw = auto_kw(k);
+    if (A->val_type == EDX_C128) {
+        EDX_REQUIRE(vec_type == EDX_C128, "spmm: a complex128 matrix needs complex128 vectors");
+        return launch_spmm_v<double2, double2>(A, k, kw, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    }
+    if (vec_type == EDX_C128) return launch_spmm_v<float2, double2>(A, k, kw, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    return launch_spmm_v<float2, float2>(A, k, kw, x, ldx_, y, ldy, ycs, al, sg, be, st);
+}
+
+}  // namespace edx
+
+using namespace edx;
+
+extern "C" int edx_spmm(const edx_csr* A, int k, int vec_type, const void* d_x, int64_t ldx_, void* d_y,
+                        int64_t ldy, double alpha_re, double alpha_im, double sigma_re, double sigma_im,
+                        double beta_re, double beta_im, int col_group, void* stream) {
+    int rc = check_csr(A);
+    if (rc) return rc;
+    EDX_REQUIRE(k >= 1, "edx_spmm: k must be >= 1");
+    EDX_REQUIRE(ldx_ >= k && ldy >= k, "edx_spmm: leading dimensions must be >= k");
+    EDX_REQUIRE(d_x != nullptr && d_y != nullptr, "edx_spmm: NULL vectors");
+    EDX_REQUIRE(vec_type == EDX_C128 || vec_type == EDX_C64, "edx_spmm: bad vec_type");
+    if ((sigma_re != 0.0 || sigma_im != 0.0))
+        EDX_REQUIRE(A->nrows == A->ncols, "edx_spmm: sigma needs a square matrix");
+    EDX_REQUIRE(col_group == 0 || col_group == 1 || col_group == 2 || col_group == 4 ||
+                    col_group == 8 || col_group == 16 || col_group == 32,
+                "edx_spmm: column group width must be a power of two <= 32");
+    if (A->nrows == 0) return EDX_OK;
+    return spmm_dispatch(A, k, vec_type, d_x, ldx_, d_y, ldy, 1, make_double2(alpha_re, alpha_im),
+                         make_double2(sigma_re, sigma_im), make_double2(beta_re, beta_im), col_group,
+                         as_stream(stream));
+}

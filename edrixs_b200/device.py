@@ -1,0 +1,306 @@
+"""Torch-facing wrappers of the libedx kernels.
+
+Tensors stay on the current CUDA device; every call runs on torch's current stream.
+Workspaces are taken from torch's caching allocator, so repeated calls do not hit
+cudaMalloc.  Nothing here has a CPU path: without a GPU and libedx.so the calls raise.
+"""
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import BuildDesc, Csr, KrylovOpts, call
+
+C128, C64 = _lib.EDX_C128, _lib.EDX_C64
+HAM_I, HAM_N, TRANS_I, TRANS_F = _lib.EDX_HAM_I, _lib.EDX_HAM_N, _lib.EDX_TRANS_I, _lib.EDX_TRANS_F
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _work(nbytes):
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
+
+
+def require_cuda():
+    if not torch.cuda.is_available():
+        raise RuntimeError("edrixs_b200 needs a CUDA device (sm_100a); no CPU path exists")
+    _lib.load()
+
+
+# ------------------------------------------------------------------------------------
+# Fock basis
+# ------------------------------------------------------------------------------------
+
+@dataclass
+class Basis:
+    """Ascending Fock states on the device (int64 holding the uint64 bit patterns)."""
+    states: torch.Tensor
+    norb: int = 0   # >0 when `states` is exactly the full norb/nelec sector
+    nelec: int = 0
+
+    @property
+    def ndim(self):
+        return int(self.states.numel())
+
+
+def fock_count(norb, nelec):
+    n = ctypes.c_int64(0)
+    call("edx_fock_count", norb, nelec, ctypes.byref(n))
+    return n.value
+
+
+def fock_unrank(norb, nelec):
+    """Full norb/nelec sector in ascending order (replaces get_fock_full_N + sort)."""
+    require_cuda()
+    n = fock_count(norb, nelec)
+    out = torch.empty(n, dtype=torch.int64, device="cuda")
+    call("edx_fock_unrank", norb, nelec, _ptr(out), n, _stream())
+    return Basis(out, norb, nelec)
+
+
+def basis_from_states(states):
+    """Wrap a sorted state list (e.g. read from fock_*.in); detects the full-sector case."""
+    require_cuda()
+    arr = np.asarray(states, dtype=np.uint64)
+    t = torch.from_numpy(arr.view(np.int64)).to("cuda")
+    b = Basis(t)
+    if len(arr) == 0:
+        return b
+    top = int(arr[-1])
+    norb = max(top.bit_length(), 1)
+    nelec = bin(int(arr[0])).count("1")
+    if norb <= 63:
+        ws = ctypes.c_size_t(0)
+        call("edx_fock_match_full_workspace", ctypes.byref(ws))
+        w = _work(ws.value)
+        full = ctypes.c_int(0)
+        call("edx_fock_match_full", norb, nelec, _ptr(t), len(arr), ctypes.byref(full), _ptr(w), ws.value,
+             _stream())
+        if full.value:
+            b.norb, b.nelec = norb, nelec
+    return b
+
+
+# ------------------------------------------------------------------------------------
+# CSR
+# ------------------------------------------------------------------------------------
+
+@dataclass
+class CSR:
+    row_ptr: torch.Tensor          # int64 [nrows+1]
+    col: torch.Tensor              # int32 [nnz]
+    val: torch.Tensor              # complex128 [nnz]
+    ncols: int
+    val64: Optional[torch.Tensor] = None  # complex64 copy (mixed-precision products)
+
+    @property
+    def nrows(self):
+        return self.row_ptr.numel() - 1
+
+    @property
+    def nnz(self):
+        return self.col.numel()
+
+    def desc(self, c64=False):
+        v = self.val64 if c64 else self.val
+        if c64 and v is None:
+            raise ValueError("this CSR has no complex64 copy")
+        return Csr(self.nrows, self.ncols, self.nnz, _ptr(self.row_ptr), _ptr(self.col), _ptr(v),
+                   C64 if c64 else C128)
+
+    def nbytes(self, c64=False):
+        return self.row_ptr.numel() * 8 + self.nnz * (4 + (8 if c64 else 16))
+
+    def to_c64(self):
+        if self.val64 is None:
+            self.val64 = self.val.to(torch.complex64)
+        return self
+
+
+def _terms_to_device(terms, nidx):
+    if terms is None:
+        return None, None, 0
+    idx, val = terms
+    idx = np.ascontiguousarray(np.asarray(idx, dtype=np.int32).reshape(-1, nidx))
+    val = np.ascontiguousarray(np.asarray(val, dtype=np.complex128).reshape(-1))
+    return (torch.from_numpy(idx).to("cuda"), torch.from_numpy(val).to("cuda"), len(val))
+
+
+def build_csr(mode, left: Basis, hopping, coulomb=None, right: Optional[Basis] = None, num_val_orbs=0,
+              num_core_orbs=0, ham_sign=1.0, omega=0j, want_c64=False):
+    """Two-pass CSR build of src/ham.f90 (see include/edx.h).  hopping/coulomb are
+    (idx 1-based, values) pairs as read from the *.in files."""
+    require_cuda()
+    hi, hv, nh = _terms_to_device(hopping, 2)
+    ci, cv, ncl = _terms_to_device(coulomb, 4)
+    search = right if mode in (TRANS_I, TRANS_F) else left
+    d = BuildDesc(mode, _ptr(left.states), left.ndim, _ptr(right.states) if right is not None else None,
+                  right.ndim if right is not None else 0, num_val_orbs, num_core_orbs, search.norb, search.nelec,
+                  nh, _ptr(hi), _ptr(hv), ncl, _ptr(ci), _ptr(cv), float(ham_sign), float(np.real(omega)),
+                  float(np.imag(omega)))
+    L = _lib.load()
+    nrows = L.edx_build_nrows(ctypes.byref(d))
+    ncols = L.edx_build_ncols(ctypes.byref(d))
+    ws = ctypes.c_size_t(0)
+    call("edx_build_workspace", ctypes.byref(d), ctypes.byref(ws))
+    sws = ctypes.c_size_t(0)
+    call("edx_build_scan_workspace", nrows, ctypes.byref(sws))
+    w = _work(max(ws.value, sws.value))
+    row_nnz = torch.empty(nrows, dtype=torch.int32, device="cuda")
+    cap = ctypes.c_int(0)
+    st = _stream()
+    call("edx_build_count", ctypes.byref(d), _ptr(row_nnz), ctypes.byref(cap), _ptr(w), ws.value, st)
+    row_ptr = torch.empty(nrows + 1, dtype=torch.int64, device="cuda")
+    nnz = ctypes.c_int64(0)
+    call("edx_build_scan", _ptr(row_nnz), nrows, _ptr(row_ptr), ctypes.byref(nnz), _ptr(w), sws.value, st)
+    del row_nnz
+    col = torch.empty(max(nnz.value, 1), dtype=torch.int32, device="cuda")[:nnz.value]
+    val = torch.empty(max(nnz.value, 1), dtype=torch.complex128, device="cuda")[:nnz.value]
+    val64 = torch.empty(max(nnz.value, 1), dtype=torch.complex64, device="cuda")[:nnz.value] if want_c64 else None
+    if nnz.value > 0:
+        call("edx_build_fill", ctypes.byref(d), cap.value, _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(val64),
+             _ptr(w), ws.value, st)
+    # the term tensors may be released now: the caching allocator only reuses their memory
+    # for work queued later on this stream, after the fill kernel
+    return CSR(row_ptr, col, val, ncols, val64)
+
+
+# ------------------------------------------------------------------------------------
+# products and solvers
+# ------------------------------------------------------------------------------------
+
+def spmm(A: CSR, X, Y=None, alpha=1.0, sigma=0.0, beta=0.0, c64=False, col_group=0):
+    """Y = alpha*(A X) + sigma*X + beta*Y; X is (ncols,) or (ncols, k) row-major."""
+    squeeze = X.dim() == 1
+    Xm = X.reshape(X.shape[0], -1)
+    k = Xm.shape[1]
+    if Y is None:
+        Y = torch.zeros((A.nrows, k), dtype=X.dtype, device=X.device)
+        beta = 0.0
+    Ym = Y.reshape(Y.shape[0], -1)
+    vec_type = C64 if X.dtype == torch.complex64 else C128
+    assert Xm.stride(1) == 1 and Ym.stride(1) == 1
+    al, sg, be = complex(alpha), complex(sigma), complex(beta)
+    call("edx_spmm", ctypes.byref(A.desc(c64)), k, vec_type, _ptr(Xm), Xm.stride(0), _ptr(Ym), Ym.stride(0),
+         al.real, al.imag, sg.real, sg.imag, be.real, be.imag, col_group, _stream())
+    return Y.reshape(-1) if squeeze else Y
+
+
+@dataclass
+class KrylovResult:
+    alpha: torch.Tensor   # (k, maxn) float64 (device)
+    beta: torch.Tensor    # (k, maxn)
+    norm: torch.Tensor    # (k,)
+    neff: torch.Tensor    # (k,) int32
+    proj: list            # per projector: (k, maxn, nrows_p) complex128
+    shift_y: Optional[torch.Tensor] = None      # (nshift, maxn) complex128
+    shift_iters: Optional[torch.Tensor] = None
+    shift_res: Optional[torch.Tensor] = None
+
+
+def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_maxit=None):
+    """k independent Lanczos recurrences (build_krylov_mp) from the columns of V0 (n, k).
+    proj: CSR operators applied to every Lanczos vector.  shifts: (col_index int array,
+    complex z array) -> per-shift MINRES coefficients in the Lanczos basis."""
+    V0 = V0.reshape(V0.shape[0], -1).contiguous()
+    n, k = V0.shape
+    dev = V0.device
+    alpha = torch.zeros((k, maxn), dtype=torch.float64, device=dev)
+    beta = torch.zeros((k, maxn), dtype=torch.float64, device=dev)
+    norm = torch.zeros(k, dtype=torch.float64, device=dev)
+    neff = torch.zeros(k, dtype=torch.int32, device=dev)
+    opts = KrylovOpts()
+    keep = []
+    outs = []
+    if proj:
+        descs = (Csr * len(proj))(*[P.desc() for P in proj])
+        outs = [torch.zeros((k, maxn, P.nrows), dtype=torch.complex128, device=dev) for P in proj]
+        ptrs = (ctypes.c_void_p * len(proj))(*[o.data_ptr() for o in outs])
+        opts.nproj = len(proj)
+        opts.proj = descs
+        opts.proj_out = ptrs
+        keep += [descs, ptrs]
+    sy = si = sr = None
+    if shifts is not None:
+        scol, sz = shifts
+        scol_t = torch.as_tensor(np.asarray(scol, dtype=np.int32), device=dev)
+        sz_t = torch.as_tensor(np.asarray(sz, dtype=np.complex128), device=dev)
+        ns = scol_t.numel()
+        sy = torch.zeros((ns, maxn), dtype=torch.complex128, device=dev)
+        si = torch.zeros(ns, dtype=torch.int32, device=dev)
+        sr = torch.zeros(ns, dtype=torch.float64, device=dev)
+        opts.nshift = ns
+        opts.shift_col = _ptr(scol_t)
+        opts.shift_z = _ptr(sz_t)
+        opts.shift_tol = float(shift_tol)
+        opts.shift_maxit = int(shift_maxit if shift_maxit is not None else maxn)
+        opts.shift_y = _ptr(sy)
+        opts.shift_iters = _ptr(si)
+        opts.shift_res = _ptr(sr)
+        keep += [scol_t, sz_t]
+    ws = ctypes.c_size_t(0)
+    call("edx_krylov_workspace", n, k, ctypes.byref(opts), maxn, ctypes.byref(ws))
+    w = _work(ws.value)
+    call("edx_krylov", ctypes.byref(A.desc(c64)), k, _ptr(V0), maxn, _ptr(alpha), _ptr(beta), _ptr(norm),
+         _ptr(neff), ctypes.byref(opts), _ptr(w), ws.value, _stream())
+    return KrylovResult(alpha, beta, norm, neff, outs, sy, si, sr)
+
+
+def minres(A: CSR, b, tol, maxit, alpha=1.0, sigma=0.0, c64=False):
+    """pminres_csr on op(A) = alpha*A + sigma*I; returns (x, iterations, |res| estimate)."""
+    n = A.nrows
+    x = torch.zeros(n, dtype=torch.complex128, device=b.device)
+    ws = ctypes.c_size_t(0)
+    call("edx_minres_workspace", n, ctypes.byref(ws))
+    w = _work(ws.value)
+    it = ctypes.c_int(0)
+    res = ctypes.c_double(0)
+    al, sg = complex(alpha), complex(sigma)
+    b = b.contiguous()
+    call("edx_minres", ctypes.byref(A.desc(c64)), al.real, al.imag, sg.real, sg.imag, _ptr(b), _ptr(x),
+         float(tol), int(maxit), ctypes.byref(it), ctypes.byref(res), _ptr(w), ws.value, _stream())
+    return x, it.value, res.value
+
+
+def cf_spectrum(neff, alpha, beta, e0, norm, weight, omega, gamma, per_set=False):
+    """Continued fraction of get_spectra_from_poles on the device.
+    alpha/beta: (nset, ld) float64; returns (ngrid,) or (nset, ngrid)."""
+    nset, ld = alpha.shape
+    dev = alpha.device
+    f64 = dict(dtype=torch.float64, device=dev)
+    omega = torch.as_tensor(omega, **f64).contiguous()
+    gamma = torch.broadcast_to(torch.as_tensor(gamma, **f64), omega.shape).contiguous()
+    out = torch.zeros((nset, omega.numel()) if per_set else (omega.numel(),), **f64)
+    # every argument tensor is bound to a name: a temporary freed before the launch could
+    # hand its memory to the next argument
+    neff_t = neff.to(torch.int32).contiguous()
+    alpha_t, beta_t = alpha.contiguous(), beta.contiguous()
+    e0_t = torch.as_tensor(np.asarray(e0, dtype=np.float64), **f64).contiguous()
+    norm_t = torch.as_tensor(np.asarray(norm, dtype=np.float64) if not torch.is_tensor(norm) else norm,
+                             **f64).contiguous()
+    w_t = torch.as_tensor(np.asarray(weight, dtype=np.float64), **f64).contiguous()
+    call("edx_cf_spectrum", nset, _ptr(neff_t), _ptr(alpha_t), _ptr(beta_t), ld, _ptr(e0_t), _ptr(norm_t),
+         _ptr(w_t), omega.numel(), _ptr(omega), _ptr(gamma), _ptr(out), 1 if per_set else 0, 0, _stream())
+    return out
+
+
+def denmat(basis: Basis, nv, vecs):
+    """<c+_i c_j> per eigenvector (ed_driver.f90:194-248): vecs (n, nvec) -> (nvec, nv, nv)."""
+    vecs = vecs.reshape(vecs.shape[0], -1).contiguous()
+    n, nvec = vecs.shape
+    out = torch.zeros((nvec, nv, nv), dtype=torch.complex128, device=vecs.device)
+    ws = ctypes.c_size_t(0)
+    call("edx_denmat_workspace", n, nv, nvec, ctypes.byref(ws))
+    w = _work(ws.value)
+    call("edx_denmat", _ptr(basis.states), n, basis.norb, basis.nelec, nv, nvec, _ptr(vecs), _ptr(out), _ptr(w),
+         ws.value, _stream())
+    return out

@@ -1,0 +1,205 @@
+/*
+ * edx.h -- C ABI of libedx, the B200 (sm_100a) exact-diagonalisation core behind the
+ * ED/XAS/RIXS solvers of EDRIXS.
+ *
+ * Plain pointers and sizes only.  Pointers named d_* are device pointers on the current
+ * CUDA device; `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ * Every function returns an EDX_* status; on failure edx_last_error() holds a message.
+ * Nothing here aborts the process (the reference STOPs instead, src/io.f90:37-39).
+ *
+ * Layouts
+ *   complex128 = two doubles (re, im); complex64 = two floats.
+ *   CSR: row_ptr int64[nrows+1] 0-based, col int32[nnz] 0-based and ascending within a
+ *   row, val complex128 or complex64[nnz].  The reference's CSR (src/m_types.f90:39-54)
+ *   is 1-based int32; subtract one from its iaa/jaa to compare.
+ *   Multi-vector blocks X are row-major: element (row r, column c) at X[r*ld + c].
+ *
+ * Workspace: entry points that need scratch take (d_work, work_bytes) from the caller and
+ * report the size they need through the matching *_workspace() query.
+ */
+#ifndef EDX_H
+#define EDX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDX_ABI_VERSION 1
+
+/* status codes */
+#define EDX_OK 0
+#define EDX_ERR_INVALID 1       /* bad argument */
+#define EDX_ERR_CUDA 2          /* a CUDA call failed */
+#define EDX_ERR_WORKSPACE 3     /* caller workspace too small */
+#define EDX_ERR_ROW_CAPACITY 4  /* a row produced more candidate entries than supported */
+#define EDX_ERR_OVERFLOW 5      /* index does not fit the index type */
+
+/* value types */
+#define EDX_C128 0
+#define EDX_C64 1
+
+/* build modes (src/ham.f90) */
+#define EDX_HAM_I 0   /* build_ham_i      src/ham.f90:2-349    */
+#define EDX_HAM_N 1   /* build_ham_n      src/ham.f90:352-711  */
+#define EDX_TRANS_I 2 /* build_transop_i  src/ham.f90:714-912  */
+#define EDX_TRANS_F 3 /* build_transop_f  src/ham.f90:915-1115 */
+
+const char* edx_last_error(void);
+int edx_abi_version(void);
+
+/* ---------------------------------------------------------------------------------- */
+/* Fock basis                                                                          */
+/* ---------------------------------------------------------------------------------- */
+
+/* Number of norb-bit states with nelec electrons, C(norb, nelec); norb <= 63. */
+int edx_fock_count(int norb, int nelec, int64_t* ndim);
+
+/* All norb-bit states with popcount nelec in ascending order, by combinatorial unranking.
+ * Replaces get_fock_full_N + sort + write/read of fock_*.in
+ * (edrixs/fock_basis.py:133-172, :398-451; src/io.f90:174-361). */
+int edx_fock_unrank(int norb, int nelec, uint64_t* d_fock, int64_t ndim, void* stream);
+
+/* *is_full = 1 if d_fock[0..ndim) is exactly the full norb/nelec basis (then column lookups
+ * may use combinatorial ranking instead of src/utils.f90:2-40 binary search). Synchronises. */
+int edx_fock_match_full(int norb, int nelec, const uint64_t* d_fock, int64_t ndim, int* is_full,
+                        void* d_work, size_t work_bytes, void* stream);
+int edx_fock_match_full_workspace(size_t* bytes);
+
+/* ---------------------------------------------------------------------------------- */
+/* Hamiltonian / transition-operator CSR build: two passes (count, then fill) exactly as   */
+/* src/ham.f90:59-188 and :213-346: per row, terms in file order (hopping, then Coulomb,  */
+/* then the omega diagonal when ham_sign < 0), fermion signs from popcounts, columns      */
+/* ascending, duplicates summed in term order, explicit zeros kept                        */
+/* (src/m_types.f90:74-121).                                                              */
+/* ---------------------------------------------------------------------------------- */
+typedef struct edx_build_desc {
+    int mode;                      /* EDX_HAM_I / EDX_HAM_N / EDX_TRANS_I / EDX_TRANS_F */
+    const uint64_t* fock_left;     /* row-side valence basis (device), ascending */
+    int64_t ndim_left;
+    const uint64_t* fock_right;    /* column-side valence basis for TRANS_I/TRANS_F */
+    int64_t ndim_right;
+    int num_val_orbs;              /* nv: core bits sit above the nv valence bits */
+    int num_core_orbs;             /* nc */
+    int search_norb, search_nelec; /* >0: the searched basis is the full set -> ranking */
+    int nhopp;                     /* two-fermion terms (hopping / transop files) */
+    const int32_t* hopp_idx;       /* device int32[2*nhopp], 1-based as in the files */
+    const double* hopp_val;        /* device complex128[nhopp] */
+    int ncoul;                     /* four-fermion terms (HAM modes only) */
+    const int32_t* coul_idx;       /* device int32[4*ncoul], 1-based */
+    const double* coul_val;        /* device complex128[ncoul] */
+    double ham_sign;               /* HAM modes: multiplies every term value */
+    double omega_re, omega_im;     /* HAM modes with ham_sign < 0: added on the diagonal */
+} edx_build_desc;
+
+int64_t edx_build_nrows(const edx_build_desc* d);
+int64_t edx_build_ncols(const edx_build_desc* d);
+int edx_build_workspace(const edx_build_desc* d, size_t* bytes);
+/* Pass 1: d_row_nnz[nrows] = merged entries per row; *cap_out = the per-row candidate
+ * capacity that the fill pass must be given.  Synchronises (reads an overflow flag). */
+int edx_build_count(const edx_build_desc* d, int32_t* d_row_nnz, int* cap_out, void* d_work,
+                    size_t work_bytes, void* stream);
+/* Exclusive scan of the row counts into d_row_ptr[nrows+1]; *h_nnz = total (synchronises). */
+int edx_build_scan(const int32_t* d_row_nnz, int64_t nrows, int64_t* d_row_ptr, int64_t* h_nnz,
+                   void* d_work, size_t work_bytes, void* stream);
+int edx_build_scan_workspace(int64_t nrows, size_t* bytes);
+/* Pass 2: columns and values at d_row_ptr[r]; d_val64 (complex64 copy) may be NULL. */
+int edx_build_fill(const edx_build_desc* d, int cap, const int64_t* d_row_ptr, int32_t* d_col,
+                   double* d_val, float* d_val64, void* d_work, size_t work_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Sparse products                                                                     */
+/* ---------------------------------------------------------------------------------- */
+typedef struct edx_csr {
+    int64_t nrows, ncols, nnz;
+    const int64_t* row_ptr;
+    const int32_t* col;
+    const void* val;
+    int val_type; /* EDX_C128 or EDX_C64 */
+} edx_csr;
+
+/* Y = alpha*(A X) + sigma*X + beta*Y over k columns (sigma needs nrows == ncols).
+ * With beta = 1, sigma = 0 this is matvec_csr's y += A x (src/spmv.f90:73-103, the
+ * per-rank kernel of pspmv_csr src/spmv.f90:1-71).  vec_type: EDX_C128 or EDX_C64 for X
+ * and Y; C64 X/Y require a C64 matrix (complex64 arithmetic).  col_group: columns handled
+ * per lane group of a warp (power of two <= 32; 0 = smallest power of two >= min(k, 32)). */
+int edx_spmm(const edx_csr* A, int k, int vec_type, const void* d_x, int64_t ldx, void* d_y,
+             int64_t ldy, double alpha_re, double alpha_im, double sigma_re, double sigma_im,
+             double beta_re, double beta_im, int col_group, void* stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Lanczos / Krylov                                                                     */
+/* ---------------------------------------------------------------------------------- */
+
+/* Optional extras of edx_krylov (pass NULL for none).
+ *
+ * Projections: every normalised Lanczos vector v_i (i = 0..maxn-1, v_0 = v0/|v0|) of every
+ *   column j is multiplied by each CSR proj[p] (e.g. an emission operator) and stored
+ *   column-major per column: proj_out[p][(j*maxn + i)*proj[p].nrows + r].
+ * Shifted solves: for each shift s (column shift_col[s], complex shift_z[s]) the MINRES
+ *   recurrence of pminres_csr (src/linsys.f90:3-128) for (z - A) x = v0_j is carried in the
+ *   Lanczos basis of A: the Lanczos vectors of z - A are +-those of A and its alpha is
+ *   z - alpha, so all shifts of one column share one Krylov space.  Each shift stops on its
+ *   own with the reference's rule (|res| <= shift_tol or iterations >= shift_maxit) and the
+ *   loop ends when every shift has stopped.  Output: x_s = sum_i shift_y[s*maxn + i] v_i
+ *   (complex128 coefficients), shift_iters[s], shift_res[s]. */
+typedef struct edx_krylov_opts {
+    int nproj;
+    const edx_csr* proj;         /* host array of nproj matrices */
+    double* const* proj_out;     /* host array of nproj device pointers */
+    int nshift;
+    const int32_t* shift_col;    /* device int32[nshift] */
+    const double* shift_z;       /* device complex128[nshift] */
+    double shift_tol;
+    int shift_maxit;
+    double* shift_y;             /* device complex128[nshift*maxn] */
+    int32_t* shift_iters;        /* device int32[nshift] */
+    double* shift_res;           /* device double[nshift] */
+} edx_krylov_opts;
+
+/* k independent Lanczos recurrences of build_krylov_mp (src/lanczos.f90:210-303), run
+ * together so that every iteration is one SpMM over k columns (FP64 recurrence).  d_v0:
+ * n x k (ld = k) start vectors.  Outputs for column j: d_alpha[j*maxn + i],
+ * d_beta[j*maxn + i] (i < neff), d_norm[j] = <v0_j|v0_j>, d_neff[j].  Column j stops when
+ * beta < 1e-10 (absolute, :291).  The matrix may be complex128 or complex64 (vectors and
+ * scalars stay complex128 / FP64). */
+int edx_krylov_workspace(int64_t n, int k, const edx_krylov_opts* opts, int maxn, size_t* bytes);
+int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn, double* d_alpha,
+               double* d_beta, double* d_norm, int32_t* d_neff, const edx_krylov_opts* opts,
+               void* d_work, size_t work_bytes, void* stream);
+
+/* MINRES of pminres_csr (src/linsys.f90:3-128) for one right-hand side, x0 = 0, with the
+ * same complex Givens recurrences and stopping rule (|res| <= tol or iter >= maxit).
+ * A is applied as alpha*(A x) + sigma*x (alpha = 1, sigma = 0 reproduces the reference,
+ * which stores omega + E_g + i*gamma - H_n explicitly; alpha = -1, sigma = z applies the
+ * same operator to a resident H_n without rebuilding it). */
+int edx_minres_workspace(int64_t n, size_t* bytes);
+int edx_minres(const edx_csr* A, double alpha_re, double alpha_im, double sigma_re,
+               double sigma_im, const double* d_b, double* d_x, double tol, int maxit,
+               int* iters_out, double* res_out, void* d_work, size_t work_bytes, void* stream);
+
+/* Continued fraction of get_spectra_from_poles (edrixs/plot_spectrum.py:41-61) for nset
+ * pole sets on one grid:  spec[w] (+)= sum_s weight[s] * norm[s] * (-1/pi) *
+ * Im 1/(x - a_1 - b_1^2/(x - a_2 - ...)),  x = omega[w] + i*gamma[w] + e0[s].
+ * Pole set s: neff[s] coefficients at d_alpha[s*ld], d_beta[s*ld].  With per_set != 0 the
+ * output is d_spec[s*ngrid + w] (no sum over s). */
+int edx_cf_spectrum(int nset, const int32_t* d_neff, const double* d_alpha, const double* d_beta,
+                    int ld, const double* d_e0, const double* d_norm, const double* d_weight,
+                    int ngrid, const double* d_omega, const double* d_gamma, double* d_spec,
+                    int per_set, int accumulate, void* stream);
+
+/* Density matrix of ed_driver.f90:194-248 for nvec eigenvectors (n x nvec, ld = nvec) over
+ * the ascending basis d_fock: d_out[(v*nv + i)*nv + j] = the reference's denmat(i+1, j+1, v+1)
+ * (complex128).  Off-diagonal terms skip rows whose amplitude is below 1e-10 as the
+ * reference does.  Deterministic (row chunks summed in order). */
+int edx_denmat_workspace(int64_t n, int nv, int nvec, size_t* bytes);
+int edx_denmat(const uint64_t* d_fock, int64_t n, int search_norb, int search_nelec, int nv,
+               int nvec, const double* d_vecs, double* d_out, void* d_work, size_t work_bytes,
+               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDX_H */

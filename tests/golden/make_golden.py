@@ -1,0 +1,273 @@
+"""Generate the golden fixtures of tests/golden from the reference's own Python layer.
+
+Run once where the reference is importable:
+    python tests/golden/make_golden.py /path/to/edrixs-reference
+
+What it writes (all small):
+  known_answer/      the case of edrixs/tests/test_fortran.py:8-42 -- config.in,
+                     hopping_i.in, coulomb_i.in, fock_i.in exactly as that test writes them,
+                     plus expected_eigvals.txt from build_opers + scipy.linalg.eigh (:14-17).
+  dense_small.npz    a 12-orbital SIAM (10 d + 2 bath, 2p core): the term lists as the files
+                     carry them and the dense matrices of H_i, H_n, D_in, D_out built by the
+                     reference's manybody_operator.two_fermion / four_fermion
+                     (edrixs/manybody_operator.py:52-176) on bases ordered like the Fortran
+                     rows (core-major intermediate index, src/ham.f90:424-446).
+  fock_digests.json  sha256 of the sorted get_fock_full_N(norb, N) arrays (int64, little
+                     endian) for the workload sizes, plus two explicit small lists.
+  spectra.npz        random pole sets and get_spectra_from_poles (edrixs/plot_spectrum.py:9-61)
+                     output on XAS/RIXS-like grids; boltz_dist (edrixs/utils.py:54-73) values.
+  siam_callers/      the exact files ed_siam_fort (do_ed=2), xas_siam_fort and rixs_siam_fort
+                     write before calling the solver (captured with a recording stand-in for
+                     edrixs.fedrixs).
+"""
+import hashlib
+import json
+import os
+import shutil
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+
+def import_reference(path):
+    mpl = types.ModuleType("matplotlib")
+    mpl.pyplot = types.ModuleType("matplotlib.pyplot")
+    sys.modules.setdefault("matplotlib", mpl)
+    sys.modules.setdefault("matplotlib.pyplot", mpl.pyplot)
+    sys.path.insert(0, path)
+    import edrixs
+    return edrixs
+
+
+class FakeComm:
+    """The four calls solvers.py makes on an mpi4py communicator."""
+
+    def Get_rank(self):
+        return 0
+
+    def Get_size(self):
+        return 1
+
+    def py2f(self):
+        return 0
+
+    def Barrier(self):
+        pass
+
+
+def bits(state, norb):
+    return np.array([(state >> p) & 1 for p in range(norb)], dtype=np.int64)
+
+
+def known_answer(ed, out):
+    os.makedirs(out, exist_ok=True)
+    norb, noccu = 10, 2
+    emat = ed.cf_cubic_d(1.5)
+    umat = ed.get_umat_slater("d", 4.0, 2.0, 0.5)
+    basis = ed.get_fock_bin_by_N(norb, noccu)
+    H = ed.build_opers(2, emat, basis) + ed.build_opers(4, umat, basis)
+    import scipy.linalg
+    e, _ = scipy.linalg.eigh(H)
+    cwd = os.getcwd()
+    os.chdir(out)
+    try:
+        with open("config.in", "w") as f:
+            f.write("&control\n"
+                    "ed_solver     =   0\n"
+                    "num_val_orbs  =   20\n"
+                    "ncv           =   150\n"
+                    f"neval         =   {len(e)}\n"
+                    f"nvector       =   {len(e)}\n"
+                    f"num_gs        =   {len(e)}\n"
+                    "maxiter       =   1000\n"
+                    "eigval_tol    =   1E-10\n"
+                    "idump         =   .true.\n"
+                    "&end\n")
+        ed.write_fock_dec_by_N(norb, noccu)
+        ed.write_emat(emat, "hopping_i.in")
+        ed.write_umat(umat, "coulomb_i.in")
+    finally:
+        os.chdir(cwd)
+    np.savetxt(os.path.join(out, "expected_eigvals.txt"), e, fmt="%.17e")
+
+
+def dense_small(ed, out_path):
+    from edrixs_b200 import siam
+    nbath, N = 2, 3
+    m = siam.make_siam(nbath, N, seed=7)
+    nv, nc = m.nv, 6
+    ntot = nv + nc
+    # what the files carry (write_emat/write_umat text, parsed back)
+    with tempfile.TemporaryDirectory() as td:
+        paths = {}
+        for name, t, fn in (("hop_i", m.emat_i, ed.write_emat), ("hop_n", m.emat_n, ed.write_emat),
+                            ("coul_i", m.umat_i, ed.write_umat), ("coul_n", m.umat_n, ed.write_umat)):
+            p = os.path.join(td, name)
+            fn(t, p)
+            paths[name] = p
+        pol_in, pol_out = siam.rixs_polarisations()[1]
+        t_in = siam.polarised_operator(m, pol_in)
+        t_out_dag = np.conj(siam.polarised_operator(m, pol_out)).T
+        ed.write_emat(t_in, os.path.join(td, "tr_i"))
+        ed.write_emat(t_out_dag, os.path.join(td, "tr_f"))
+
+        def load(p, nidx):
+            with open(p) as f:
+                n = int(f.readline().split()[0])
+                rows = [f.readline().split() for _ in range(n)]
+            idx = np.array([[int(r[k]) for k in range(nidx)] for r in rows], dtype=np.int32)
+            val = np.array([float(r[nidx]) + 1j * float(r[nidx + 1]) for r in rows])
+            return idx, val
+
+        hi, ci = load(paths["hop_i"], 2), load(paths["coul_i"], 4)
+        hn, cn = load(paths["hop_n"], 2), load(paths["coul_n"], 4)
+        ti, tf = load(os.path.join(td, "tr_i"), 2), load(os.path.join(td, "tr_f"), 2)
+
+    def tensor2(terms, n):
+        t = np.zeros((n, n), dtype=complex)
+        for (i, j), v in zip(terms[0], terms[1]):
+            t[i - 1, j - 1] += v
+        return t
+
+    def tensor4(terms, n):
+        t = np.zeros((n,) * 4, dtype=complex)
+        for (i, j, k, l), v in zip(terms[0], terms[1]):
+            t[i - 1, j - 1, k - 1, l - 1] += v
+        return t
+
+    fock_i = np.array(sorted(ed.get_fock_full_N(nv, N)), dtype=np.int64)
+    fock_n = np.array(sorted(ed.get_fock_full_N(nv, N + 1)), dtype=np.int64)
+    core_full = (1 << nc) - 1
+    fock_core = [core_full - (1 << (nc - 1 - k)) for k in range(nc)]
+    basis_i = [bits(s, nv) for s in fock_i]                                  # valence only
+    basis_i_fullcore = [bits((core_full << nv) | s, ntot) for s in fock_i]   # with the core
+    basis_n = [bits((fc << nv) | s, ntot) for fc in fock_core for s in fock_n]
+    # H_i acts on valence-only states in build_ham_i: restrict the tensors to nv orbitals
+    H_i = (ed.two_fermion(tensor2(hi, ntot)[:nv, :nv], basis_i) +
+           ed.four_fermion(tensor4(ci, ntot)[:nv, :nv, :nv, :nv], basis_i))
+    H_n = ed.two_fermion(tensor2(hn, ntot), basis_n) + ed.four_fermion(tensor4(cn, ntot), basis_n)
+    D_in = ed.two_fermion(tensor2(ti, ntot), basis_n, basis_i_fullcore)
+    D_out = ed.two_fermion(tensor2(tf, ntot), basis_i_fullcore, basis_n)
+
+    def coo(Mx):
+        r, c = np.nonzero(Mx)
+        return r.astype(np.int32), c.astype(np.int32), Mx[r, c]
+
+    data = dict(nv=nv, nc=nc, nelec=N, fock_i=fock_i, fock_n=fock_n,
+                hop_i_idx=hi[0], hop_i_val=hi[1], coul_i_idx=ci[0], coul_i_val=ci[1],
+                hop_n_idx=hn[0], hop_n_val=hn[1], coul_n_idx=cn[0], coul_n_val=cn[1],
+                tr_i_idx=ti[0], tr_i_val=ti[1], tr_f_idx=tf[0], tr_f_val=tf[1])
+    for name, Mx in (("H_i", H_i), ("H_n", H_n), ("D_in", D_in), ("D_out", D_out)):
+        r, c, v = coo(Mx)
+        data[f"{name}_row"], data[f"{name}_col"], data[f"{name}_val"] = r, c, v
+        data[f"{name}_shape"] = np.array(Mx.shape)
+    np.savez_compressed(out_path, **data)
+    return {k: v.shape for k, v in data.items() if hasattr(v, "shape")}
+
+
+def fock_digests(ed, out_path):
+    res = {}
+    for norb, N in ((20, 10), (20, 11), (24, 12), (26, 13)):
+        a = np.array(sorted(ed.get_fock_full_N(norb, N)), dtype="<i8")
+        res[f"{norb}_{N}"] = {"ndim": int(len(a)), "sha256": hashlib.sha256(a.tobytes()).hexdigest(),
+                              "first": [int(x) for x in a[:3]], "last": [int(x) for x in a[-3:]]}
+    res["explicit_4_2"] = [int(x) for x in sorted(ed.get_fock_full_N(4, 2))]
+    res["explicit_6_3"] = [int(x) for x in sorted(ed.get_fock_full_N(6, 3))]
+    with open(out_path, "w") as f:
+        json.dump(res, f, indent=1)
+
+
+def spectra(ed, out_path):
+    rng = np.random.default_rng(11)
+    poles = {"npoles": [], "eigval": [], "norm": [], "alpha": [], "beta": []}
+    for g in range(3):
+        neff = [40, 200, 1][g]
+        poles["npoles"].append(neff)
+        poles["eigval"].append(float(-12.3 + 0.01 * g))
+        poles["norm"].append(float(rng.uniform(0.5, 2.0)))
+        poles["alpha"].append(list(rng.uniform(-15, 5, neff)))
+        poles["beta"].append(list(rng.uniform(0.1, 3.0, neff)))
+    om_xas = np.linspace(-5, 15, 1000)
+    om_rixs = np.linspace(-1, 12, 2000)
+    gam_rixs = np.linspace(0.1, 0.4, 2000)
+    s_xas = ed.get_spectra_from_poles(poles, om_xas, np.full(1000, 0.3), 300.0)
+    s_rixs = ed.get_spectra_from_poles(poles, om_rixs, gam_rixs, 10.0)
+    np.savez_compressed(out_path, npoles=np.array(poles["npoles"]), eigval=np.array(poles["eigval"]),
+                        norm=np.array(poles["norm"]),
+                        alpha=np.array([np.pad(a, (0, 200 - len(a))) for a in poles["alpha"]]),
+                        beta=np.array([np.pad(b, (0, 200 - len(b))) for b in poles["beta"]]),
+                        om_xas=om_xas, s_xas=s_xas, om_rixs=om_rixs, gam_rixs=gam_rixs, s_rixs=s_rixs,
+                        boltz_e=np.array([-3.0, -2.99, -2.5]), boltz_T=np.array([1.0, 300.0, 3000.0]),
+                        boltz=np.array([ed.boltz_dist([-3.0, -2.99, -2.5], T) for T in (1.0, 300.0, 3000.0)]))
+
+
+def siam_callers(ed, out_dir):
+    """Record what the reference's callers write for the solver (tiny model: 10 d + 2 bath)."""
+    from edrixs_b200 import siam
+    m = siam.make_siam(2, 3, seed=7)
+    hopping = m.emat_i[:m.nv, :m.nv]
+    slater = ([8.0, 10.0, 6.2], [8.0, 10.0, 6.2] + list(siam.DEFAULT_SLATER_VC))
+    calls = {"n": 0}
+
+    def recorder(kind):
+        def fsolver(comm, my_id, num_procs):
+            calls["n"] += 1
+            d = os.path.join(out_dir, f"{kind}_{calls['n']}")
+            os.makedirs(d, exist_ok=True)
+            for fn in os.listdir("."):
+                if fn.endswith(".in"):
+                    shutil.copy(fn, os.path.join(d, fn))
+            # minimal outputs so that the caller can go on
+            if kind == "xas" or kind == "rixs":
+                for g in range(1):
+                    with open(f"{kind}_poles.{g + 1}", "w") as f:
+                        f.write("#number_of_poles:            1\n#enegry:                  0.0\n"
+                                "#normalization:           1.0\n    1      0.0      0.0\n")
+        return fsolver
+
+    mod = types.ModuleType("edrixs.fedrixs")
+    mod.ed_fsolver = recorder("ed")
+    mod.xas_fsolver = recorder("xas")
+    mod.rixs_fsolver = recorder("rixs")
+    sys.modules["edrixs.fedrixs"] = mod
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as td:
+        os.chdir(td)
+        try:
+            comm = FakeComm()
+            ed.ed_siam_fort(comm, ("d", "p"), 0, siam_type=1, v_noccu=3, hopping=m.emat_i[:10, :10],
+                            slater=slater, c_soc=11.0, do_ed=2, ed_solver=2, neval=4, nvector=2, ncv=20,
+                            idump=True, maxiter=1000, eigval_tol=1e-10, min_ndim=10)
+            d = os.path.join(out_dir, "ed_do_ed2")
+            os.makedirs(d, exist_ok=True)
+            for fn in os.listdir("."):
+                if fn.endswith(".in"):
+                    shutil.copy(fn, os.path.join(d, fn))
+            ed.xas_siam_fort(comm, ("d", "p"), 0, np.linspace(-2, 8, 11), gamma_c=0.3, v_noccu=3,
+                             pol_type=[("linear", 0.0)], num_gs=1, nkryl=50, temperature=300.0)
+            ed.rixs_siam_fort(comm, ("d", "p"), 0, np.array([1.5]), np.linspace(-0.5, 5, 11), gamma_c=0.6,
+                              gamma_f=0.1, v_noccu=3, pol_type=[("linear", 0.0, "linear", np.pi / 2)],
+                              num_gs=1, nkryl=50, linsys_max=500, linsys_tol=1e-10, temperature=300.0)
+        finally:
+            os.chdir(cwd)
+    del hopping
+
+
+def main(ref):
+    ed = import_reference(ref)
+    known_answer(ed, os.path.join(HERE, "known_answer"))
+    print("dense_small", dense_small(ed, os.path.join(HERE, "dense_small.npz")))
+    fock_digests(ed, os.path.join(HERE, "fock_digests.json"))
+    spectra(ed, os.path.join(HERE, "spectra.npz"))
+    siam_callers(ed, os.path.join(HERE, "siam_callers"))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,156 @@
+"""Pin the CPU oracle to the reference: golden vectors made by the reference's own code.
+
+* Fock bases == get_fock_full_N (sorted) digests at the workload sizes.
+* CSR build == the reference's dense builder (manybody_operator.two_fermion/four_fermion)
+  entry for entry, for H_i, H_n (core-hole sector), D_in and D_out.
+* The known-answer ED case of edrixs/tests/test_fortran.py.
+* Continued-fraction spectra and Boltzmann weights == get_spectra_from_poles / boltz_dist.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as orc
+
+
+def test_fock_small_lists(golden_dir):
+    d = json.load(open(os.path.join(golden_dir, "fock_digests.json")))
+    assert list(orc.fock_full_N(4, 2)) == d["explicit_4_2"]
+    assert list(orc.fock_full_N(6, 3)) == d["explicit_6_3"]
+
+
+@pytest.mark.parametrize("norb,N", [(20, 10), (20, 11), (24, 12), (26, 13)])
+def test_fock_digest(golden_dir, norb, N):
+    d = json.load(open(os.path.join(golden_dir, "fock_digests.json")))[f"{norb}_{N}"]
+    a = orc.fock_full_N(norb, N).astype("<i8")
+    assert len(a) == d["ndim"]
+    assert hashlib.sha256(a.tobytes()).hexdigest() == d["sha256"]
+
+
+def test_binary_search_semantics():
+    v = orc.fock_full_N(6, 3)
+    for i, s in enumerate(v):
+        assert orc.binary_search(v, s) == i + 1
+    assert orc.binary_search(v, 1) == -1
+    assert orc.binary_search(v, 1 << 40) == -1
+
+
+def _dense_from_coo(g, name):
+    shape = tuple(g[f"{name}_shape"])
+    M = np.zeros(shape, dtype=complex)
+    M[g[f"{name}_row"], g[f"{name}_col"]] = g[f"{name}_val"]
+    return M
+
+
+def _close(A, B, rtol=1e-13):
+    scale = max(np.abs(B).max(), 1.0)
+    return np.abs(A - B).max() <= rtol * scale
+
+
+def test_build_ham_i_matches_reference_dense(dense_small):
+    g = dense_small
+    csr = orc.build_csr("ham_i", g["fock_i"], (g["hop_i_idx"], g["hop_i_val"]), (g["coul_i_idx"], g["coul_i_val"]),
+                        num_val_orbs=int(g["nv"]))
+    ref = _dense_from_coo(g, "H_i")
+    assert _close(csr.dense(), ref)
+    # rows sorted ascending, no duplicate columns
+    for r in range(csr.nrows):
+        c = csr.col[csr.row_ptr[r]:csr.row_ptr[r + 1]]
+        assert np.all(np.diff(c) > 0)
+
+
+def test_build_ham_n_matches_reference_dense(dense_small):
+    g = dense_small
+    csr = orc.build_csr("ham_n", g["fock_n"], (g["hop_n_idx"], g["hop_n_val"]), (g["coul_n_idx"], g["coul_n_val"]),
+                        num_val_orbs=int(g["nv"]), num_core_orbs=int(g["nc"]))
+    assert csr.nrows == 6 * len(g["fock_n"])
+    assert _close(csr.dense(), _dense_from_coo(g, "H_n"))
+
+
+def test_build_transop_i_matches_reference_dense(dense_small):
+    g = dense_small
+    csr = orc.build_csr("trans_i", g["fock_n"], (g["tr_i_idx"], g["tr_i_val"]), fock_right=g["fock_i"],
+                        num_val_orbs=int(g["nv"]), num_core_orbs=int(g["nc"]))
+    assert _close(csr.dense(), _dense_from_coo(g, "D_in"))
+
+
+def test_build_transop_f_matches_reference_dense(dense_small):
+    g = dense_small
+    csr = orc.build_csr("trans_f", g["fock_i"], (g["tr_f_idx"], g["tr_f_val"]), fock_right=g["fock_n"],
+                        num_val_orbs=int(g["nv"]), num_core_orbs=int(g["nc"]))
+    assert _close(csr.dense(), _dense_from_coo(g, "D_out"))
+
+
+def test_omega_diagonal_and_sign(dense_small):
+    """ham_sign = -1 with omega: A = omega*I - H exactly (rixs_driver.f90:130-133)."""
+    g = dense_small
+    H = orc.build_csr("ham_n", g["fock_n"], (g["hop_n_idx"], g["hop_n_val"]), (g["coul_n_idx"], g["coul_n_val"]),
+                      num_val_orbs=int(g["nv"]), num_core_orbs=int(g["nc"]))
+    z = 3.25 + 0.6j
+    A = orc.build_csr("ham_n", g["fock_n"], (g["hop_n_idx"], g["hop_n_val"]), (g["coul_n_idx"], g["coul_n_val"]),
+                      num_val_orbs=int(g["nv"]), num_core_orbs=int(g["nc"]), ham_sign=-1.0, omega=z)
+    assert np.allclose(A.dense(), z * np.eye(A.nrows) - H.dense(), atol=1e-13)
+    # every row carries the diagonal
+    for r in range(A.nrows):
+        assert r in A.col[A.row_ptr[r]:A.row_ptr[r + 1]]
+
+
+def test_known_answer_eigenvalues(golden_dir):
+    """edrixs/tests/test_fortran.py:8-42 through the oracle (ZHEEV path)."""
+    d = os.path.join(golden_dir, "known_answer")
+    fock = orc.read_fock(os.path.join(d, "fock_i.in"))
+    hop = orc.read_terms(os.path.join(d, "hopping_i.in"), 2)
+    coul = orc.read_terms(os.path.join(d, "coulomb_i.in"), 4)
+    csr = orc.build_csr("ham_i", fock, hop, coul, num_val_orbs=20)
+    e = np.linalg.eigvalsh(csr.dense())
+    expected = np.loadtxt(os.path.join(d, "expected_eigvals.txt"))
+    assert np.all(np.isclose(e, expected))
+    assert np.abs(e - expected).max() < 1e-10
+
+
+def test_spectra_and_boltzmann(golden_dir):
+    with np.load(os.path.join(golden_dir, "spectra.npz")) as z:
+        g = {k: z[k] for k in z.files}
+    poles = {"npoles": list(g["npoles"]), "eigval": list(g["eigval"]), "norm": list(g["norm"]),
+             "alpha": [list(a) for a in g["alpha"]], "beta": [list(b) for b in g["beta"]]}
+    s = orc.spectra_from_poles(poles, g["om_xas"], 0.3, 300.0)
+    assert np.abs(s - g["s_xas"]).max() <= 1e-12 * np.abs(g["s_xas"]).max()
+    s = orc.spectra_from_poles(poles, g["om_rixs"], g["gam_rixs"], 10.0)
+    assert np.abs(s - g["s_rixs"]).max() <= 1e-12 * np.abs(g["s_rixs"]).max()
+    for T, w in zip(g["boltz_T"], g["boltz"]):
+        assert np.allclose(orc.boltz_dist(g["boltz_e"], T), w, rtol=1e-14, atol=0)
+
+
+def test_matvec_krylov_minres_consistency(dense_small):
+    """Oracle SpMV / Krylov / MINRES against dense numpy algebra on the same matrix."""
+    g = dense_small
+    H = orc.build_csr("ham_n", g["fock_n"], (g["hop_n_idx"], g["hop_n_val"]), (g["coul_n_idx"], g["coul_n_val"]),
+                      num_val_orbs=int(g["nv"]), num_core_orbs=int(g["nc"]))
+    Hd = H.dense()
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=H.nrows) + 1j * rng.normal(size=H.nrows)
+    assert np.allclose(orc.matvec(H, x), Hd @ x, rtol=1e-13, atol=1e-12)
+    a, b, nrm, neff = orc.build_krylov(H, x, 20)
+    assert neff == 20 and abs(nrm - np.vdot(x, x).real) < 1e-9
+    # first alpha is the Rayleigh quotient of the start vector
+    assert abs(a[0] - np.vdot(x, Hd @ x).real / np.vdot(x, x).real) < 1e-9
+    z = 40.0 + 0.6j
+    A = orc.build_csr("ham_n", g["fock_n"], (g["hop_n_idx"], g["hop_n_val"]), (g["coul_n_idx"], g["coul_n_val"]),
+                      num_val_orbs=int(g["nv"]), num_core_orbs=int(g["nc"]), ham_sign=-1.0, omega=z)
+    sol, it, res = orc.minres(A, x, 1e-10, 2000)
+    exact = np.linalg.solve(A.dense(), x)
+    assert np.abs(sol - exact).max() / np.abs(exact).max() < 1e-8
+    assert res <= 1e-10
+
+
+def test_denmat_oracle_trace(dense_small):
+    g = dense_small
+    H = orc.build_csr("ham_i", g["fock_i"], (g["hop_i_idx"], g["hop_i_val"]), (g["coul_i_idx"], g["coul_i_val"]),
+                      num_val_orbs=int(g["nv"]))
+    e, v = np.linalg.eigh(H.dense())
+    dm = orc.denmat(g["fock_i"], int(g["nv"]), v[:, 0])
+    assert abs(np.trace(dm).real - int(g["nelec"])) < 1e-10
+    assert np.allclose(dm, dm.conj().T, atol=1e-10)

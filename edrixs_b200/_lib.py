@@ -45,7 +45,10 @@ class Csr(ctypes.Structure):
 class KrylovOpts(ctypes.Structure):
     _fields_ = [("nproj", ctypes.c_int), ("proj", ctypes.POINTER(Csr)), ("proj_out", ctypes.POINTER(vp)),
                 ("nshift", ctypes.c_int), ("shift_col", vp), ("shift_z", vp), ("shift_tol", dbl),
-                ("shift_maxit", ctypes.c_int), ("shift_y", vp), ("shift_iters", vp), ("shift_res", vp)]
+                ("shift_maxit", ctypes.c_int), ("shift_y", vp), ("shift_iters", vp), ("shift_res", vp),
+                ("apply_ms", ctypes.POINTER(ctypes.c_double)), ("apply_launches", ctypes.POINTER(ctypes.c_int)),
+                ("apply_col_group", ctypes.c_int), ("apply_threads", ctypes.c_int),
+                ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int)]
 
 
 _SIGS = {

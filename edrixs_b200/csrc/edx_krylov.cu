@@ -36,10 +36,10 @@ __device__ __forceinline__ bool arrive_last(unsigned* ticket) {
 
 // Sum a per-thread value over threads of the block that share local column c (there are
 // `groups` of them, laid out as sh[g*KW + c]); result written to part[bx*k + gc].
-template <int KW>
+template <int KW, int NT = KT>
 __device__ __forceinline__ void block_col_partial(double v, bool writer, int g, int groups, int c, int k,
                                                   double* part) {
-    __shared__ double sh[KT];
+    __shared__ double sh[NT];
     if (writer) sh[g * KW + c] = v;
     __syncthreads();
     if (threadIdx.x < KW) {
@@ -71,11 +71,16 @@ struct KrylovState {
 };
 
 // ---- K9a: W = A V_cur - beta_{i-1} V_prev (into V_prev), alpha partials ---------------
-template <int KW, class VT>
-__global__ void __launch_bounds__(KT) k_lanczos_apply(int64_t n, const int64_t* __restrict__ row_ptr,
+// Row mapping: interleaved (warp w of block b takes rows w + NW*(b + B*i)) or chunked (block
+// b owns one contiguous range of rows).  Chunked keeps a block inside the contiguous row
+// ranges that share the high (bath) bits of the Fock states, where the impurity-internal
+// terms (Coulomb, spin-orbit, crystal field) land; their gathers then hit L1.
+template <int KW, class VT, int NT>
+__global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* __restrict__ row_ptr,
                                                       const int32_t* __restrict__ col, const VT* __restrict__ val,
                                                       const double2* __restrict__ Vc, double2* __restrict__ Vp,
-                                                      KrylovState S, int it) {
+                                                      KrylovState S, int it, int chunked) {
+    constexpr int NW = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c = lane % KW;
     const int k = S.k;
@@ -83,9 +88,18 @@ __global__ void __launch_bounds__(KT) k_lanczos_apply(int64_t n, const int64_t* 
     const bool colok = gc < k;
     const double bprev = (colok && it > 0) ? S.beta[gc] : 0.0;
     double apart = 0.0;
-    const int64_t warp0 = (int64_t)blockIdx.x * (KT / 32) + warp;
-    const int64_t nw = (int64_t)gridDim.x * (KT / 32);
-    for (int64_t r = warp0; r < n; r += nw) {
+    int64_t r0, r1, rstep;
+    if (chunked) {
+        const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+        r0 = (int64_t)blockIdx.x * per + warp;
+        r1 = min(n, (int64_t)(blockIdx.x + 1) * per);
+        rstep = NW;
+    } else {
+        r0 = (int64_t)blockIdx.x * NW + warp;
+        r1 = n;
+        rstep = (int64_t)gridDim.x * NW;
+    }
+    for (int64_t r = r0; r < r1; r += rstep) {
         const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
         double2 acc = row_times_x<KW, VT, double2>(s, e, col, val, Vc, k, gc, colok);
         if (lane < KW && colok) {
@@ -99,9 +113,9 @@ __global__ void __launch_bounds__(KT) k_lanczos_apply(int64_t n, const int64_t* 
             apart += vc.x * w.x + vc.y * w.y;  // Re(conj(v) w)
         }
     }
-    block_col_partial<KW>(apart, lane < KW, warp, KT / 32, c, k, S.part);
+    block_col_partial<KW, NT>(apart, lane < KW, warp, NW, c, k, S.part);
     if (arrive_last(S.ticket)) {
-        for (int j = threadIdx.x; j < k; j += KT) {
+        for (int j = threadIdx.x; j < k; j += NT) {
             double a = sum_partials(S.part, gridDim.x, k, j);
             S.alpha[j] = a;
             if (S.active[j]) S.alpha_out[(int64_t)j * S.maxn + it] = a;
@@ -301,28 +315,52 @@ __global__ void k_shift_final(int nshift, const ShiftState* __restrict__ st, int
     if (res) res[s] = st[s].res;
 }
 
-template <int KW, class VT>
-static int launch_apply(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
-                        int gx, cudaStream_t st) {
-    dim3 grid(gx, (S.k + KW - 1) / KW);
-    k_lanczos_apply<KW, VT><<<grid, KT, 0, st>>>(A->nrows, A->row_ptr, A->col,
-                                                 reinterpret_cast<const VT*>(A->val), Vc, Vp, S, it);
+// launch shape of the fused apply kernel (chosen by the caller's autotuner, or defaults)
+struct ApplyCfg {
+    int kw;         // columns per lane group
+    int threads;    // 256, 512 or 1024
+    int gx;         // blocks along the rows
+    int chunked;    // contiguous row ranges per block
+};
+
+template <int KW, class VT, int NT>
+static int launch_apply_nt(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+                           const ApplyCfg& cfg, cudaStream_t st) {
+    auto kern = k_lanczos_apply<KW, VT, NT>;
+    static bool carve_set = false;  // prefer L1 over shared memory: gathers are served from L1
+    if (!carve_set) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+        carve_set = true;
+    }
+    dim3 grid(cfg.gx, (S.k + KW - 1) / KW);
+    kern<<<grid, NT, 0, st>>>(A->nrows, A->row_ptr, A->col, reinterpret_cast<const VT*>(A->val), Vc, Vp, S, it,
+                              cfg.chunked);
     EDX_CHECK_LAUNCH();
     return EDX_OK;
 }
 
-template <class VT>
-static int apply_v(int kw, const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
-                   int gx, cudaStream_t st) {
-    switch (kw) {
-    case 1: return launch_apply<1, VT>(A, Vc, Vp, S, it, gx, st);
-    case 2: return launch_apply<2, VT>(A, Vc, Vp, S, it, gx, st);
-    case 4: return launch_apply<4, VT>(A, Vc, Vp, S, it, gx, st);
-    case 8: return launch_apply<8, VT>(A, Vc, Vp, S, it, gx, st);
-    case 16: return launch_apply<16, VT>(A, Vc, Vp, S, it, gx, st);
-    case 32: return launch_apply<32, VT>(A, Vc, Vp, S, it, gx, st);
+template <int KW, class VT>
+static int launch_apply(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+                        const ApplyCfg& cfg, cudaStream_t st) {
+    switch (cfg.threads) {
+    case 512: return launch_apply_nt<KW, VT, 512>(A, Vc, Vp, S, it, cfg, st);
+    case 1024: return launch_apply_nt<KW, VT, 1024>(A, Vc, Vp, S, it, cfg, st);
+    default: return launch_apply_nt<KW, VT, 256>(A, Vc, Vp, S, it, cfg, st);
     }
-    return fail(EDX_ERR_INVALID, "krylov: bad column group %d", kw);
+}
+
+template <class VT>
+static int apply_v(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+                   const ApplyCfg& cfg, cudaStream_t st) {
+    switch (cfg.kw) {
+    case 1: return launch_apply<1, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 2: return launch_apply<2, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 4: return launch_apply<4, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 8: return launch_apply<8, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 16: return launch_apply<16, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 32: return launch_apply<32, VT>(A, Vc, Vp, S, it, cfg, st);
+    }
+    return fail(EDX_ERR_INVALID, "krylov: bad column group %d", cfg.kw);
 }
 
 #define EDX_KW_SWITCH(kw, KERNEL, GRID, ...)                                                  \
@@ -396,8 +434,7 @@ using namespace edx;
 extern "C" int edx_krylov_workspace(int64_t n, int k, const edx_krylov_opts* opts, int maxn, size_t* bytes) {
     EDX_REQUIRE(bytes != nullptr && n >= 1 && k >= 1 && maxn >= 1, "edx_krylov_workspace: bad arguments");
     SizeOnly s;
-    int gx = reduce_grid(n);
-    if (gx < num_sms() * 4) gx = num_sms() * 4;  // the apply kernel's grid can be larger
+    const int gx = num_sms() * 8;  // largest grid any kernel here uses
     krylov_layout(s, n, k, opts ? opts->nshift : 0, maxn, gx, nullptr);
     *bytes = s.s.bytes();
     return EDX_OK;
@@ -423,9 +460,20 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     }
     cudaStream_t st = as_stream(stream);
     const int64_t n = A->nrows;
-    const int kw = auto_kw(k);
+    ApplyCfg cfg;
+    cfg.kw = (opts && opts->apply_col_group > 0) ? opts->apply_col_group : auto_kw(k);
+    cfg.threads = (opts && opts->apply_threads > 0) ? opts->apply_threads : 256;
+    const int bps = (opts && opts->apply_blocks_per_sm > 0) ? opts->apply_blocks_per_sm : 4;
+    cfg.chunked = (opts && opts->apply_chunked > 0) ? 1 : 0;
+    EDX_REQUIRE(cfg.kw == 1 || cfg.kw == 2 || cfg.kw == 4 || cfg.kw == 8 || cfg.kw == 16 || cfg.kw == 32,
+                "edx_krylov: apply_col_group must be a power of two <= 32");
+    EDX_REQUIRE(cfg.threads == 256 || cfg.threads == 512 || cfg.threads == 1024,
+                "edx_krylov: apply_threads must be 256, 512 or 1024");
+    EDX_REQUIRE(bps >= 1 && bps * cfg.threads <= 8 * 256, "edx_krylov: apply_blocks_per_sm out of range");
+    cfg.gx = num_sms() * bps;
+    const int kw = cfg.kw;
     const int gy = (k + kw - 1) / kw;
-    int gx = num_sms() * 4;
+    const int gx = num_sms() * 8;
     Workspace w(d_work, work_bytes);
     KrylovWs ws;
     krylov_layout(w, n, k, nshift, maxn, gx, &ws);
@@ -479,11 +527,31 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     double2* Vc = ws.Vc;
     double2* Vp = ws.Vp;
     const int poll = 8;
+    const bool timed = opts && opts->apply_ms;
+    std::vector<cudaEvent_t> evs;
+    auto drop_events = [&]() {
+        for (auto e : evs) cudaEventDestroy(e);
+        evs.clear();
+    };
+    int launches = 0;
     for (int it = 0; it < maxn; ++it) {
         if (nshift > 0) EDX_CUDA(cudaMemsetAsync(ws.n_open, 0, sizeof(int), st));
-        rc = (A->val_type == EDX_C128) ? apply_v<double2>(kw, A, Vc, Vp, S, it, gx, st)
-                                       : apply_v<float2>(kw, A, Vc, Vp, S, it, gx, st);
-        if (rc) return rc;
+        if (timed) {
+            cudaEvent_t e0, e1;
+            EDX_CUDA(cudaEventCreate(&e0));
+            EDX_CUDA(cudaEventCreate(&e1));
+            evs.push_back(e0);
+            evs.push_back(e1);
+            EDX_CUDA(cudaEventRecord(e0, st));
+        }
+        rc = (A->val_type == EDX_C128) ? apply_v<double2>(A, Vc, Vp, S, it, cfg, st)
+                                       : apply_v<float2>(A, Vc, Vp, S, it, cfg, st);
+        if (rc) {
+            drop_events();
+            return rc;
+        }
+        if (timed) EDX_CUDA(cudaEventRecord(evs.back(), st));
+        ++launches;
         {
             dim3 grid(reduce_grid(n), gy);
             EDX_KW_SWITCH(kw, k_lanczos_orth, grid, n, Vc, Vp, S, it);
@@ -510,6 +578,19 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     if (nshift > 0) {
         k_shift_final<<<(nshift + 127) / 128, 128, 0, st>>>(nshift, ws.sst, opts->shift_iters, opts->shift_res);
         EDX_CHECK_LAUNCH();
+    }
+    if (timed) {
+        EDX_CUDA(cudaStreamSynchronize(st));
+        double total = 0.0;
+        for (size_t q = 0; q + 1 < evs.size(); q += 2) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, evs[q], evs[q + 1]) == cudaSuccess) total += ms;
+        }
+        drop_events();
+        *opts->apply_ms = total;
+        if (opts->apply_launches) *opts->apply_launches = launches;
+    } else if (opts && opts->apply_launches) {
+        *opts->apply_launches = launches;
     }
     return EDX_OK;
 }

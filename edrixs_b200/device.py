@@ -207,7 +207,8 @@ class KrylovResult:
     shift_res: Optional[torch.Tensor] = None
 
 
-def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_maxit=None):
+def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_maxit=None, timing=False,
+           apply=None):
     """k independent Lanczos recurrences (build_krylov_mp) from the columns of V0 (n, k).
     proj: CSR operators applied to every Lanczos vector.  shifts: (col_index int array,
     complex z array) -> per-shift MINRES coefficients in the Lanczos basis."""
@@ -247,12 +248,25 @@ def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, s
         opts.shift_iters = _ptr(si)
         opts.shift_res = _ptr(sr)
         keep += [scol_t, sz_t]
+    if apply:
+        opts.apply_col_group = int(apply.get("col_group", 0))
+        opts.apply_threads = int(apply.get("threads", 0))
+        opts.apply_blocks_per_sm = int(apply.get("blocks_per_sm", 0))
+        opts.apply_chunked = int(apply.get("chunked", 0))
+    ms = ctypes.c_double(0.0)
+    nl = ctypes.c_int(0)
+    if timing:
+        opts.apply_ms = ctypes.pointer(ms)
+    opts.apply_launches = ctypes.pointer(nl)
     ws = ctypes.c_size_t(0)
     call("edx_krylov_workspace", n, k, ctypes.byref(opts), maxn, ctypes.byref(ws))
     w = _work(ws.value)
     call("edx_krylov", ctypes.byref(A.desc(c64)), k, _ptr(V0), maxn, _ptr(alpha), _ptr(beta), _ptr(norm),
          _ptr(neff), ctypes.byref(opts), _ptr(w), ws.value, _stream())
-    return KrylovResult(alpha, beta, norm, neff, outs, sy, si, sr)
+    res = KrylovResult(alpha, beta, norm, neff, outs, sy, si, sr)
+    res.apply_ms = ms.value if timing else None
+    res.apply_launches = nl.value
+    return res
 
 
 def minres(A: CSR, b, tol, maxit, alpha=1.0, sigma=0.0, c64=False):

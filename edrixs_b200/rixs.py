@@ -63,14 +63,23 @@ class RixsResult:
     iters: np.ndarray        # MINRES iterations per (pol_in, gs, omega)
     res: np.ndarray          # |res| estimates
     krylov_steps: int        # Lanczos steps taken on H_n
+    stats: dict = field(default_factory=dict)  # kernel launch counts and timings
 
 
 def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, linsys_tol=1e-10,
-                 linsys_max=1000, temperature=300.0, c64=False, final_block=None):
+                 linsys_max=1000, temperature=300.0, c64=False, final_block=None, timing=False, autotune=False):
     omegas = np.asarray(omegas, dtype=np.float64)
     eloss = np.asarray(eloss, dtype=np.float64)
     n_om, ne = len(omegas), len(eloss)
     npin, npout, ngs = len(P.Din), len(P.Dout), len(P.gs_e)
+    k_hn = npin * ngs
+    K_hf = npout * k_hn * n_om if final_block is None else int(final_block)
+    if autotune:
+        from . import tune
+        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64)
+        P.meta[("apply", "hf", K_hf, c64)] = tune.tune_apply(P.Hf, K_hf, c64=c64)
+    cfg_hn = P.meta.get(("apply", "hn", k_hn, c64))
+    cfg_hf = P.meta.get(("apply", "hf", K_hf, c64))
     gam_c = np.broadcast_to(np.asarray(gamma_c, dtype=np.float64), (n_om,))
     dev = P.gs_v.device
     # 1. seeds (n_n, npin*ngs), column c = p_in*ngs + g
@@ -83,9 +92,15 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     maxn = int(linsys_max)
     # 3. one Krylov space per seed + projections through every D_out^+
     r = device.krylov(P.Hn, seeds, maxn, c64=c64, proj=P.Dout, shifts=(scol, sz), shift_tol=linsys_tol,
-                      shift_maxit=linsys_max)
+                      shift_maxit=linsys_max, timing=timing, apply=cfg_hn)
     steps = int(r.neff.max().item())
     m = max(int(r.shift_iters.max().item()), 1)
+    iters = r.shift_iters.view(k, n_om).cpu().numpy()
+    resid = r.shift_res.view(k, n_om).cpu().numpy()
+    it_n = r.apply_launches
+    # libedx launches on H_n: 4 setup + per iteration (apply, orth, shift step, scale, projections)
+    stats = dict(hn_iterations=it_n, hn_apply_ms=r.apply_ms, hn_nnz=P.Hn.nnz, hn_rows=P.Hn.nrows, k_hn=k,
+                 launches=len(P.Din) + 4 + npout + it_n * (4 + npout))
     Y = r.shift_y.view(k, n_om, -1)[:, :, :m]                     # (k, n_om, m)
     # phi[p_out][c, w, :] = sum_i Y[c, w, i] * (D_out^+ v_i)[:]
     phis = []
@@ -104,10 +119,16 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     B = torch.zeros_like(A)
     NRM = torch.zeros(K, dtype=torch.float64, device=dev)
     NEFF = torch.zeros(K, dtype=torch.int32, device=dev)
+    hf_ms, hf_it = 0.0, 0
     for s in range(0, K, blk):
         e = min(K, s + blk)
-        rf = device.krylov(P.Hf, V0[:, s:e].contiguous(), nkryl, c64=c64)
+        rf = device.krylov(P.Hf, V0[:, s:e].contiguous(), nkryl, c64=c64, timing=timing, apply=cfg_hf)
         A[s:e], B[s:e], NRM[s:e], NEFF[s:e] = rf.alpha, rf.beta, rf.norm, rf.neff
+        hf_ms += rf.apply_ms or 0.0
+        hf_it += rf.apply_launches
+        stats["launches"] += 2 + 3 * rf.apply_launches
+    stats.update(hf_apply_ms=hf_ms if timing else None, hf_iterations=hf_it, hf_nnz=P.Hf.nnz, hf_rows=P.Hf.nrows,
+                 k_hf=blk)
     del V0
     # 5. continued fractions; column order (p_out, p_in, g, w)
     e0 = np.tile(np.repeat(np.tile(P.gs_e, npin), n_om), npout)
@@ -115,10 +136,18 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
                               np.broadcast_to(np.asarray(gamma_f, dtype=np.float64), (ne,)), per_set=True)
     spec = spec.view(npout, npin, ngs, n_om, ne)
     w = torch.from_numpy(boltz(P.gs_e, temperature)).to(dev)
-    out = torch.einsum("oigwe,g->wieo", spec, w).reshape(n_om, ne, npin * npout)
-    iters = r_iters = None  # noqa: F841
-    return RixsResult(out.cpu().numpy(), dict(alpha=A, beta=B, norm=NRM, neff=NEFF, e0=e0),
-                      np.zeros(0), np.zeros(0), steps)
+    out = torch.einsum("oigwe,g->weio", spec, w).reshape(n_om, ne, npin * npout)
+    stats["launches"] += 1
+    return RixsResult(out.cpu().numpy(), dict(alpha=A, beta=B, norm=NRM, neff=NEFF, e0=e0), iters, resid, steps,
+                      stats)
+
+
+def rixs_request(P: RixsProblem, gs_v_host, omegas, gamma_c, eloss, gamma_f, **kw):
+    """A request as a client makes it: ground-state vectors and grids in host memory,
+    spectra back in host memory.  The vectors are copied from pinned host buffers into the
+    resident problem before the solve."""
+    P.gs_v.copy_(gs_v_host, non_blocking=True)
+    return rixs_spectra(P, omegas, gamma_c, eloss, gamma_f, **kw)
 
 
 def rixs_plain(P: RixsProblem, omega, gamma_c, eloss, gamma_f, *, pin=0, pout=0, g=0, nkryl=150, linsys_tol=1e-10,

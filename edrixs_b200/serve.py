@@ -1,0 +1,342 @@
+"""Continuous-batching request loop for ED / XAS / RIXS jobs on one GPU.
+
+* Requests name a Hamiltonian by its generating parameters (``ModelSpec``); the server keeps
+  each Hamiltonian's CSR matrices, transition operators and ground states resident in HBM
+  (``Resident``) and reuses them for later requests.
+* Admission: a request starts when its estimated device footprint (its resident problem if
+  not cached yet + its solve working set) fits in the HBM budget next to everything in
+  flight; idle residents are evicted least-recently-used to make room.  Requests that do
+  not fit wait; requests larger than the whole budget fail at admission.
+* Coalescing: waiting RIXS requests on the same Hamiltonian with the same broadening and
+  solver settings are merged into one multi-shift solve over the union of their incident
+  energies (their shifts share Krylov spaces), then split back per request.
+* Continuous batching: several worker threads, each with its own CUDA stream, run admitted
+  work concurrently; a request that arrives while others run is admitted as soon as memory
+  and a worker free up.  Every request records its queueing and service latency.
+"""
+import itertools
+import math
+import queue
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import device, rixs, siam, solvers
+
+KB = 8.6173303e-5
+
+
+@dataclass(frozen=True)
+class ModelSpec:
+    """A seeded SIAM Hamiltonian: 10 impurity + nbath bath valence orbitals, 2p core."""
+    nbath: int
+    nelec: int
+    seed: int
+
+    @property
+    def nv(self):
+        return 10 + self.nbath
+
+
+@dataclass
+class Request:
+    kind: str                      # "ed", "xas" or "rixs"
+    model: ModelSpec
+    ngs: int = 1                   # ground states used (lowest ngs)
+    omegas: Optional[np.ndarray] = None   # rixs: incident energies relative to the edge
+    eloss: Optional[np.ndarray] = None    # rixs: energy-loss grid; xas: absorption grid
+    gamma_c: float = 0.6
+    gamma_f: float = 0.1
+    pols: tuple = (0,)             # rixs: indices into siam.rixs_polarisations(); xas: xas polvec index
+    nkryl: int = 150
+    linsys_tol: float = 1e-10
+    linsys_max: int = 1000
+    temperature: float = 300.0
+    id: int = field(default_factory=lambda: next(_ids))
+    t_submit: float = 0.0
+    t_start: float = 0.0
+    t_done: float = 0.0
+
+
+_ids = itertools.count()
+
+
+class Resident:
+    """Device state of one Hamiltonian, built on first use."""
+
+    def __init__(self, spec: ModelSpec):
+        self.spec = spec
+        self.lock = threading.Lock()
+        self.Hi = None
+        self.Hn = None
+        self.bi = self.bn = None
+        self.terms = None
+        self.model = None
+        self.gs_e = None
+        self.gs_v = None
+        self.edge = None
+        self.ops = {}
+        self.busy = 0
+        self.last_used = time.monotonic()
+
+    def nbytes(self):
+        b = 0
+        for M in [self.Hi, self.Hn] + list(self.ops.values()):
+            if M is not None:
+                b += M.nbytes()
+        if self.gs_v is not None:
+            b += self.gs_v.numel() * 16
+        return b
+
+    def ensure(self, need_n=False, ngs=1):
+        with self.lock:
+            s = self.spec
+            if self.model is None:
+                self.model = siam.make_siam(s.nbath, s.nelec, s.seed)
+                m, rt = self.model, siam.text_roundtrip
+                self.terms = dict(hop_i=rt(siam.nonzero_terms(m.emat_i), 2), coul_i=rt(siam.nonzero_terms(m.umat_i), 4),
+                                  hop_n=rt(siam.nonzero_terms(m.emat_n), 2), coul_n=rt(siam.nonzero_terms(m.umat_n), 4))
+            if self.Hi is None:
+                self.bi = device.fock_unrank(s.nv, s.nelec)
+                self.Hi = device.build_csr(device.HAM_I, self.bi, self.terms["hop_i"], self.terms["coul_i"],
+                                           num_val_orbs=s.nv)
+            if self.gs_v is None or self.gs_v.shape[1] < ngs:
+                e, v = solvers.lowest_eigs(self.Hi, ngs, ngs, tol=1e-9)
+                self.gs_e, self.gs_v = np.asarray(e), v.contiguous()
+            if need_n and self.Hn is None:
+                self.bn = device.fock_unrank(s.nv, s.nelec + 1)
+                self.Hn = device.build_csr(device.HAM_N, self.bn, self.terms["hop_n"], self.terms["coul_n"],
+                                           num_val_orbs=s.nv, num_core_orbs=6)
+                e_n, _ = solvers.lowest_eigs(self.Hn, 1, 1, tol=1e-6)
+                self.edge = float(e_n[0] - self.gs_e[0])
+            # the resident is shared with other workers' streams: finish building it here
+            torch.cuda.current_stream().synchronize()
+            self.last_used = time.monotonic()
+
+    def op(self, kind, pol):
+        key = (kind, pol)
+        with self.lock:
+            if key not in self.ops:
+                m, rt, s = self.model, siam.text_roundtrip, self.spec
+                pols = siam.rixs_polarisations()
+                if kind == "in":
+                    t = rt(siam.nonzero_terms(siam.polarised_operator(m, pols[pol][0])), 2)
+                    self.ops[key] = device.build_csr(device.TRANS_I, self.bn, t, right=self.bi, num_val_orbs=s.nv,
+                                                     num_core_orbs=6)
+                elif kind == "out":
+                    t = rt(siam.nonzero_terms(np.conj(siam.polarised_operator(m, pols[pol][1])).T), 2)
+                    self.ops[key] = device.build_csr(device.TRANS_F, self.bi, t, right=self.bn, num_val_orbs=s.nv,
+                                                     num_core_orbs=6)
+                else:  # xas
+                    t = rt(siam.nonzero_terms(siam.polarised_operator(m, siam.atomic()["xas_polvec"][pol])), 2)
+                    self.ops[key] = device.build_csr(device.TRANS_I, self.bn, t, right=self.bi, num_val_orbs=s.nv,
+                                                     num_core_orbs=6)
+                torch.cuda.current_stream().synchronize()
+            return self.ops[key]
+
+
+def _dims(spec: ModelSpec):
+    ni = math.comb(spec.nv, spec.nelec)
+    nn = 6 * math.comb(spec.nv, spec.nelec + 1)
+    return ni, nn
+
+
+def estimate_bytes(req: Request, resident_cached: bool):
+    """Upper estimate of the device bytes a request needs (resident part + working set)."""
+    ni, nn = _dims(req.model)
+    per_row = 24 * 80  # ~80 nonzeros per row at 20 bytes + slack
+    resident = 0 if resident_cached else (ni + (nn if req.kind != "ed" else 0)) * per_row
+    if req.kind == "ed":
+        work = 3 * 48 * ni * 16
+    elif req.kind == "xas":
+        work = 4 * nn * 16 * max(req.ngs, 1)
+    else:
+        n_om = len(req.omegas)
+        k = len(set(p for p in req.pols)) * req.ngs
+        K = len(req.pols) * req.ngs * n_om
+        work = (2 * k * req.linsys_max * ni + 4 * nn * k + 4 * ni * K) * 16
+    return int(resident + work)
+
+
+class Server:
+    def __init__(self, hbm_budget=150e9, workers=2):
+        self.budget = float(hbm_budget)
+        self.workers = workers
+        self.residents = {}
+        self.waiting = []            # [(req, future)]
+        self.inflight_bytes = 0
+        self.cv = threading.Condition()
+        self.jobs = queue.Queue()
+        self.stop_flag = False
+        self.records = []
+        self.threads = []
+
+    # -- public ---------------------------------------------------------------------------
+    def start(self):
+        device.require_cuda()
+        self.sched = threading.Thread(target=self._schedule, daemon=True)
+        self.sched.start()
+        for i in range(self.workers):
+            t = threading.Thread(target=self._work, args=(i,), daemon=True)
+            t.start()
+            self.threads.append(t)
+        return self
+
+    def submit(self, req: Request) -> Future:
+        fut = Future()
+        req.t_submit = time.perf_counter()
+        if estimate_bytes(req, False) > self.budget:
+            fut.set_exception(MemoryError(f"request {req.id} needs more than the HBM budget"))
+            return fut
+        with self.cv:
+            self.waiting.append((req, fut))
+            self.cv.notify_all()
+        return fut
+
+    def shutdown(self):
+        with self.cv:
+            self.stop_flag = True
+            self.cv.notify_all()
+        for _ in self.threads:
+            self.jobs.put(None)
+        for t in self.threads:
+            t.join(timeout=60)
+
+    def latency_summary(self):
+        lat = np.array([r["latency_s"] for r in self.records]) if self.records else np.zeros(1)
+        return {"n": len(self.records), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3)}
+
+    # -- scheduling -----------------------------------------------------------------------
+    def _resident(self, spec):
+        if spec not in self.residents:
+            self.residents[spec] = Resident(spec)
+        return self.residents[spec]
+
+    def _resident_bytes(self):
+        return sum(r.nbytes() for r in self.residents.values())
+
+    def _evict_for(self, need):
+        idle = sorted((r for r in self.residents.values() if r.busy == 0), key=lambda r: r.last_used)
+        for r in idle:
+            if self._resident_bytes() + self.inflight_bytes + need <= self.budget:
+                break
+            del self.residents[r.spec]
+
+    def _schedule(self):
+        while True:
+            with self.cv:
+                if self.stop_flag:
+                    return
+                picked = None
+                for i, (req, fut) in enumerate(self.waiting):
+                    cached = req.model in self.residents
+                    need = estimate_bytes(req, cached)
+                    if self._resident_bytes() + self.inflight_bytes + need > self.budget:
+                        self._evict_for(need)
+                    if self._resident_bytes() + self.inflight_bytes + need <= self.budget:
+                        picked = i
+                        break
+                if picked is None:
+                    self.cv.wait(timeout=0.05)
+                    continue
+                req, fut = self.waiting.pop(picked)
+                group = [(req, fut)]
+                if req.kind == "rixs":  # coalesce waiting RIXS on the same Hamiltonian and settings
+                    sig = (req.model, req.ngs, req.gamma_c, req.gamma_f, tuple(req.pols), req.nkryl, req.linsys_tol,
+                           req.linsys_max, req.temperature, len(req.eloss), float(req.eloss[0]), float(req.eloss[-1]))
+                    rest = []
+                    for r2, f2 in self.waiting:
+                        s2 = (r2.model, r2.ngs, r2.gamma_c, r2.gamma_f, tuple(r2.pols), r2.nkryl, r2.linsys_tol,
+                              r2.linsys_max, r2.temperature, len(r2.eloss), float(r2.eloss[0]),
+                              float(r2.eloss[-1])) if r2.kind == "rixs" else None
+                        if s2 == sig:
+                            group.append((r2, f2))
+                        else:
+                            rest.append((r2, f2))
+                    self.waiting = rest
+                need = sum(estimate_bytes(r, r.model in self.residents) for r, _ in group)
+                res = self._resident(req.model)
+                res.busy += 1
+                self.inflight_bytes += need
+            self.jobs.put((group, res, need))
+
+    def _work(self, idx):
+        stream = torch.cuda.Stream()
+        while True:
+            job = self.jobs.get()
+            if job is None:
+                return
+            group, res, need = job
+            t0 = time.perf_counter()
+            try:
+                with torch.cuda.stream(stream):
+                    outs = self._run(group, res)
+                    stream.synchronize()
+                t1 = time.perf_counter()
+                for (req, fut), out in zip(group, outs):
+                    req.t_start, req.t_done = t0, t1
+                    self.records.append({"id": req.id, "kind": req.kind, "latency_s": t1 - req.t_submit,
+                                         "service_s": t1 - t0, "coalesced": len(group)})
+                    fut.set_result(out)
+            except Exception as e:  # a failed job fails its requests, never the server
+                for req, fut in group:
+                    if not fut.done():
+                        fut.set_exception(e)
+            finally:
+                with self.cv:
+                    res.busy -= 1
+                    self.inflight_bytes -= need
+                    self.cv.notify_all()
+
+    # -- solves ---------------------------------------------------------------------------
+    def _run(self, group, res: Resident):
+        req = group[0][0]
+        if req.kind == "ed":
+            res.ensure(False, req.ngs)
+            return [{"eigvals": res.gs_e[:r.ngs].copy()} for r, _ in group]
+        res.ensure(True, req.ngs)
+        if req.kind == "xas":
+            return [self._xas(r, res) for r, _ in group]
+        # union of incident energies (absolute) over the coalesced requests
+        oms = [np.asarray(r.omegas, dtype=np.float64) + res.edge for r, _ in group]
+        allw = np.unique(np.concatenate(oms))
+        pins = sorted(set(siam_pol_in(p) for p in req.pols))
+        pouts = sorted(set(siam_pol_out(p) for p in req.pols))
+        P = rixs.RixsProblem(Hn=res.Hn, Hf=res.Hi, Din=[res.op("in", p) for p in pins],
+                             Dout=[res.op("out", p) for p in pouts], gs_e=res.gs_e[:req.ngs],
+                             gs_v=res.gs_v[:, :req.ngs].contiguous())
+        out = rixs.rixs_spectra(P, allw, req.gamma_c, req.eloss, req.gamma_f, nkryl=req.nkryl,
+                                linsys_tol=req.linsys_tol, linsys_max=req.linsys_max, temperature=req.temperature)
+        results = []
+        for (r, _), om in zip(group, oms):
+            idx = np.searchsorted(allw, om)
+            cols = [pins.index(siam_pol_in(p)) * len(pouts) + pouts.index(siam_pol_out(p)) for p in r.pols]
+            results.append({"omegas": om, "spectra": out.spectra[idx][:, :, cols], "coalesced": len(group),
+                            "minres_iters": out.iters})
+        return results
+
+    def _xas(self, r: Request, res: Resident):
+        D = res.op("xas", r.pols[0])
+        phi = device.spmm(D, res.gs_v[:, :r.ngs].contiguous())
+        kr = device.krylov(res.Hn, phi, r.nkryl)
+        w = rixs.boltz(res.gs_e[:r.ngs], r.temperature)
+        grid = np.asarray(r.eloss, dtype=np.float64) + res.edge
+        spec = device.cf_spectrum(kr.neff, kr.alpha, kr.beta, res.gs_e[:r.ngs], kr.norm.cpu().numpy(), w, grid,
+                                  np.full(len(grid), r.gamma_c))
+        return {"grid": grid, "spectrum": spec.cpu().numpy()}
+
+
+def siam_pol_in(p):
+    """Incident polarisation of rixs_polarisations()[p]: entries 0,1 share pi, 2,3 share sigma."""
+    return 0 if p in (0, 1) else 2
+
+
+def siam_pol_out(p):
+    """Outgoing polarisation of rixs_polarisations()[p]: entries 0,2 share pi, 1,3 share sigma."""
+    return 0 if p in (0, 2) else 1

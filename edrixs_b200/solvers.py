@@ -28,7 +28,9 @@ def _qr(W):
 
 def dense_eigs(H: device.CSR, nev):
     n = H.nrows
-    Hd = torch.sparse_csr_tensor(H.row_ptr, H.col.to(torch.int64), H.val, size=(n, H.ncols)).to_dense()
+    rows = torch.repeat_interleave(torch.arange(n, device=H.val.device), H.row_ptr[1:] - H.row_ptr[:-1])
+    Hd = torch.zeros((n, H.ncols), dtype=H.val.dtype, device=H.val.device)
+    Hd[rows, H.col.to(torch.int64)] = H.val
     e, v = torch.linalg.eigh(Hd)  # ZHEEV('V','U') of full_diag.f90 uses the upper triangle; H is Hermitian
     return e[:nev].cpu().numpy(), v[:, :nev].contiguous()
 

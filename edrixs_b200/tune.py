@@ -1,0 +1,46 @@
+"""Autotuner for the launch shape of the fused SpMM + Lanczos-step kernel.
+
+For a given resident matrix and column count it runs a few Lanczos steps per candidate
+shape (columns per lane group, threads per block, blocks per SM, interleaved or chunked
+row mapping), times the apply launches with the CUDA events libedx records on the launch
+stream, and keeps the fastest.  Results are cached per (matrix, columns, precision).
+"""
+import torch
+
+from . import device
+
+_cache = {}
+
+
+def candidates(k):
+    kws = [0] if k <= 32 else [32, 16]
+    shapes = [(256, 4), (256, 8), (512, 2), (512, 4), (1024, 1), (1024, 2)]
+    out = []
+    for kw in kws:
+        for th, bps in shapes:
+            for ch in (0, 1):
+                out.append(dict(col_group=kw, threads=th, blocks_per_sm=bps, chunked=ch))
+    return out
+
+
+def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False):
+    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64))
+    if key in _cache:
+        return _cache[key]
+    g = torch.Generator(device=A.val.device)
+    g.manual_seed(1)
+    V0 = torch.randn((A.nrows, k), dtype=torch.float64, device=A.val.device, generator=g).to(torch.complex128)
+    best, best_t = None, float("inf")
+    results = []
+    for cfg in candidates(k):
+        r = device.krylov(A, V0, steps, c64=c64, timing=True, apply=cfg)
+        t = r.apply_ms / max(r.apply_launches, 1)
+        results.append((t, cfg))
+        if t < best_t:
+            best, best_t = cfg, t
+    del V0
+    if verbose:
+        for t, cfg in sorted(results, key=lambda x: x[0]):
+            print(f"  {t * 1e3:9.1f} us  {cfg}")
+    _cache[key] = dict(best, ms_per_launch=best_t)
+    return _cache[key]

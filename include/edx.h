@@ -157,6 +157,18 @@ typedef struct edx_krylov_opts {
     double* shift_y;             /* device complex128[nshift*maxn] */
     int32_t* shift_iters;        /* device int32[nshift] */
     double* shift_res;           /* device double[nshift] */
+    /* optional instrumentation (host pointers, may be NULL): total device time of the fused
+     * SpMM + recurrence launches (the dominant kernel), measured with CUDA events recorded
+     * on `stream` around each launch, and the number of those launches */
+    double* apply_ms;
+    int* apply_launches;
+    /* launch shape of the fused SpMM + recurrence kernel (0 = default): columns per lane
+     * group (power of two <= 32), threads per block (256/512/1024), blocks per SM, and the
+     * row mapping (0 = interleaved rows, 1 = one contiguous row range per block) */
+    int apply_col_group;
+    int apply_threads;
+    int apply_blocks_per_sm;
+    int apply_chunked;
 } edx_krylov_opts;
 
 /* k independent Lanczos recurrences of build_krylov_mp (src/lanczos.f90:210-303), run

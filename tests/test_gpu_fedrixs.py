@@ -1,0 +1,163 @@
+"""End-to-end drop-in parity: edrixs_b200.fedrixs on the reference's own input files vs the
+oracle drivers; batched RIXS vs the reference's per-(omega, pol, gs) loop.
+
+Tolerances: eigenvalues <= 1e-10 eV; spectra <= 1e-6 relative L-inf
+(max |S - S_ref| / max |S_ref|), each against the FP64 oracle.
+"""
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+from oracle import drivers as odrv
+from oracle import pyoracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_linf(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / np.abs(np.asarray(b)).max())
+
+
+def _spectrum(poles_list, grid, gamma, T=300.0):
+    poles = {"npoles": [p[3] for p in poles_list], "eigval": [p[4] for p in poles_list],
+             "norm": [p[2] for p in poles_list], "alpha": [list(p[0]) for p in poles_list],
+             "beta": [list(p[1]) for p in poles_list]}
+    return orc.spectra_from_poles(poles, grid, gamma, T)
+
+
+def _as_written(poles_list, tmpdir):
+    """The oracle's poles as the reference's write_krylov would store them (f20.10 fields)."""
+    from edrixs_b200 import io
+    out = []
+    for i, (a, b, nrm, neff, e) in enumerate(poles_list[:]):
+        p = os.path.join(tmpdir, f"oracle_poles.{i + 1}")
+        io.write_poles(p, neff, a, b, nrm, e)
+        pd = io.read_poles([p])
+        out.append((np.array(pd["alpha"][0]), np.array(pd["beta"][0]), pd["norm"][0], pd["npoles"][0],
+                    pd["eigval"][0]))
+    return out
+
+
+def _read_our_poles(d, prefix, num_gs):
+    from edrixs_b200 import io
+    pd = io.read_poles([os.path.join(d, f"{prefix}.{i + 1}") for i in range(num_gs)])
+    return [(np.array(pd["alpha"][i]), np.array(pd["beta"][i]), pd["norm"][i], pd["npoles"][i], pd["eigval"][i])
+            for i in range(num_gs)]
+
+
+@pytest.fixture
+def workdir(tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    return tmp_path
+
+
+def test_ed_known_answer(cuda, golden_dir, workdir):
+    """edrixs/tests/test_fortran.py:8-42 through the drop-in ed_fsolver (ed_solver = 0)."""
+    from edrixs_b200 import fedrixs
+    for f in os.listdir(os.path.join(golden_dir, "known_answer")):
+        shutil.copy(os.path.join(golden_dir, "known_answer", f), workdir)
+    fedrixs.ed_fsolver(0, 0, 1)
+    _, e = np.loadtxt("eigvals.dat", unpack=True)
+    expected = np.loadtxt("expected_eigvals.txt")
+    assert np.all(np.isclose(e, expected))
+    assert np.abs(e - expected).max() < 1e-9  # file carries 10 decimals
+    assert len(np.loadtxt("denmat.dat")) == 45 * 20 * 20
+    assert os.path.exists("eigvec.45")
+
+
+def test_ed_thick_restart_lanczos(cuda, workdir):
+    """ed_solver = 2 (ARPACK in the reference) -> block thick-restart Lanczos, 12870 states."""
+    from edrixs_b200 import fedrixs, io, siam
+    m = siam.make_siam(6, 8, seed=21)
+    siam.write_ed_inputs(m, str(workdir), neval=4, nvector=2, ed_solver=2, eigval_tol=1e-10)
+    fedrixs.ed_fsolver(0, 0, 1)
+    e_ref, v_ref, H, fock, cfg = odrv.ed(str(workdir))
+    e_ours = np.loadtxt("eigvals.dat")[:, 1]
+    assert np.abs(e_ours - e_ref).max() < 2e-10
+    # unrounded values from the eigenvector files
+    e1, v1 = io.read_eigvec("eigvec.1")
+    assert abs(e1 - e_ref[0]) < 1e-10
+    # eigenvector: residual and overlap with the oracle ground state (phase-free)
+    Hv = orc.matvec(H, v1)
+    assert np.linalg.norm(Hv - e1 * v1) < 1e-7
+    if e_ref[1] - e_ref[0] > 1e-6:
+        assert abs(abs(np.vdot(v_ref[:, 0], v1)) - 1.0) < 1e-10
+        dm_ref = odrv.denmat(fock, cfg["num_val_orbs"], v_ref[:, :1])[0]
+        dm = np.loadtxt("denmat.dat")
+        ours = (dm[: 16 * 16, 3] + 1j * dm[: 16 * 16, 4]).reshape(16, 16)
+        assert np.abs(ours - dm_ref).max() < 1e-9
+
+
+def _ed_then(golden_dir, workdir, kind):
+    """Run our ED on the reference callers' ED files, then stage the XAS/RIXS files."""
+    from edrixs_b200 import fedrixs
+    src = os.path.join(golden_dir, "siam_callers")
+    for f in os.listdir(os.path.join(src, "ed_do_ed2")):
+        shutil.copy(os.path.join(src, "ed_do_ed2", f), workdir)
+    fedrixs.ed_fsolver(0, 0, 1)
+    sub = [d for d in os.listdir(src) if d.startswith(kind)][0]
+    for f in os.listdir(os.path.join(src, sub)):
+        shutil.copy(os.path.join(src, sub, f), workdir)
+
+
+def test_xas_drop_in(cuda, golden_dir, workdir):
+    from edrixs_b200 import fedrixs
+    _ed_then(golden_dir, workdir, "xas")
+    fedrixs.xas_fsolver(0, 0, 1)
+    ref = _as_written(odrv.xas(str(workdir)), str(workdir))
+    ours = _read_our_poles(str(workdir), "xas_poles", len(ref))
+    grid = np.linspace(-10, 30, 1000)
+    s_ref, s = _spectrum(ref, grid, 0.3), _spectrum(ours, grid, 0.3)
+    assert rel_linf(s, s_ref) < 1e-6
+
+
+def test_rixs_drop_in(cuda, golden_dir, workdir):
+    from edrixs_b200 import fedrixs
+    _ed_then(golden_dir, workdir, "rixs")
+    fedrixs.rixs_fsolver(0, 0, 1)
+    ref = _as_written([r[:5] for r in odrv.rixs(str(workdir))], str(workdir))
+    ours = _read_our_poles(str(workdir), "rixs_poles", len(ref))
+    grid = np.linspace(-0.5, 12, 2000)
+    s_ref, s = _spectrum(ref, grid, 0.1), _spectrum(ours, grid, 0.1)
+    assert rel_linf(s, s_ref) < 1e-6
+
+
+def test_rixs_batched_matches_reference_loop(cuda):
+    """All omega x pol_in x pol_out x gs from shared Krylov spaces == the per-point loop."""
+    import torch
+    from edrixs_b200 import device, rixs, siam
+    m = siam.make_siam(2, 3, seed=4)
+    nv, N = m.nv, 3
+    t = dict(hop_i=siam.text_roundtrip(siam.nonzero_terms(m.emat_i), 2),
+             coul_i=siam.text_roundtrip(siam.nonzero_terms(m.umat_i), 4),
+             hop_n=siam.text_roundtrip(siam.nonzero_terms(m.emat_n), 2),
+             coul_n=siam.text_roundtrip(siam.nonzero_terms(m.umat_n), 4))
+    pols = siam.rixs_polarisations()
+    din = [siam.text_roundtrip(siam.nonzero_terms(siam.polarised_operator(m, pols[p][0])), 2) for p in (0, 3)]
+    dout = [siam.text_roundtrip(siam.nonzero_terms(np.conj(siam.polarised_operator(m, pols[p][1])).T), 2)
+            for p in (0, 3)]
+    fi = orc.fock_full_N(nv, N)
+    Hi = orc.build_csr("ham_i", fi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
+    e, v = np.linalg.eigh(Hi.dense())
+    gs_e, gs_v = e[:2], np.ascontiguousarray(v[:, :2])
+    Hn_ref = orc.build_csr("ham_n", orc.fock_full_N(nv, N + 1), t["hop_n"], t["coul_n"], num_val_orbs=nv,
+                           num_core_orbs=6)
+    e_n = np.linalg.eigvalsh(Hn_ref.dense())
+    edge = e_n[0] - gs_e[0]
+    omegas = edge + np.array([0.5, 2.0, 4.5])
+    eloss = np.linspace(-0.5, 8, 300)
+    ref = odrv.rixs_in_memory(t, nv, N, gs_e, gs_v, din, dout, omegas, 0.6, eloss, 0.1, 60, 1e-10, 1000, 300.0)
+    bi = device.fock_unrank(nv, N)
+    bn = device.fock_unrank(nv, N + 1)
+    P = rixs.RixsProblem(
+        Hn=device.build_csr(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6),
+        Hf=device.build_csr(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=nv),
+        Din=[device.build_csr(device.TRANS_I, bn, d, right=bi, num_val_orbs=nv, num_core_orbs=6) for d in din],
+        Dout=[device.build_csr(device.TRANS_F, bi, d, right=bn, num_val_orbs=nv, num_core_orbs=6) for d in dout],
+        gs_e=gs_e, gs_v=torch.from_numpy(gs_v).cuda())
+    res = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, nkryl=60, linsys_tol=1e-10, linsys_max=1000,
+                            temperature=300.0)
+    assert res.spectra.shape == ref.shape
+    assert rel_linf(res.spectra, ref) < 1e-6

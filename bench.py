@@ -44,7 +44,32 @@ def parse():
     ap.add_argument("--c64", action="store_true", help="complex64 matrices in the Krylov products")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--kernel-case", choices=["apply"], default=None,
+                    help="run only a small profiling case of the dominant kernels (for ncu)")
     return ap.parse_args()
+
+
+def kernel_case(args):
+    """The apply kernels on this workload's matrices, two launches each (a few GB on the
+    device): H_n with the 6 seed columns, H_f with 256 final-state columns, and one SpMV of
+    the one-RHS MINRES.  Launch shapes are the autotuner's usual winners."""
+    import torch
+    from edrixs_b200 import device
+    m, t = workload_terms(args.nbath, args.nelec)
+    nv, N = m.nv, args.nelec
+    bi, bn = device.fock_unrank(nv, N), device.fock_unrank(nv, N + 1)
+    Hf = device.build_csr(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
+    Hn = device.build_csr(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    V = torch.randn((Hn.nrows, 6), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    device.krylov(Hn, V, 2, apply=dict(threads=1024, blocks_per_sm=1, chunked=1))
+    W = torch.randn((Hf.nrows, 256), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=4, threads=1024, blocks_per_sm=1, chunked=1))
+    b = torch.randn(Hn.nrows, dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    device.minres(Hn, b, 1e-300, 1, alpha=-1.0, sigma=40 + 0.6j)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": "apply", "nnz_Hn": Hn.nnz, "nnz_Hf": Hf.nnz}))
 
 
 def load_peaks():
@@ -186,22 +211,10 @@ def cpu_sample(args, t, gs, omega, iters_minres, minres_its=60, krylov_steps=60)
 # arms
 # ------------------------------------------------------------------------------------
 
-def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    return ws, rank
-
-
 def run_ours(args):
     import torch
-    from edrixs_b200 import rixs
-    ws, rank = dist_init()
+    from edrixs_b200 import dist, rixs
+    ws, rank = dist.init_from_env()
     dev_index = torch.cuda.current_device()
     m, t, P, omegas, eloss = setup_gpu(args)
     kw = dict(nkryl=args.nkryl, linsys_tol=1e-10, linsys_max=1000, temperature=300.0, c64=args.c64)
@@ -212,10 +225,7 @@ def run_ours(args):
     tuned = {f"{k[1]}_k{k[2]}": {kk: v for kk, v in cfg.items() if kk != "ms_per_launch"}
              for k, cfg in P.meta.items() if isinstance(k, tuple) and k[0] == "apply"}
 
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
+    barrier = dist.barrier
 
     # device-resident timed region
     lat = []
@@ -238,11 +248,7 @@ def run_ours(args):
         barrier()
     total_ms = ev0.elapsed_time(ev1)
     lat_ms = [a.elapsed_time(b) for a, b in lat]
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = dist.reduce_max(total_ms)
     n_om = len(omegas)
     value = ws * n_om * args.steps / (total_ms / 1e3)
 
@@ -257,12 +263,7 @@ def run_ours(args):
         out = rixs.rixs_request(P, gs_host, omegas, 0.6, eloss, 0.1, **kw)
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = dist.reduce_max(e0.elapsed_time(e1))
     e2e_value = ws * n_om * args.steps / (e2e_ms / 1e3)
     h2d = gs_host.numel() * 16 + omegas.nbytes + eloss.nbytes
     d2h = out.spectra.nbytes
@@ -352,9 +353,7 @@ def run_ours(args):
         }
         line.update(extra)
         print(json.dumps(line), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    dist.finalize()
 
 
 def run_reference(args):
@@ -392,7 +391,9 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.kernel_case:
+        kernel_case(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

@@ -48,7 +48,8 @@ class KrylovOpts(ctypes.Structure):
                 ("shift_maxit", ctypes.c_int), ("shift_y", vp), ("shift_iters", vp), ("shift_res", vp),
                 ("apply_ms", ctypes.POINTER(ctypes.c_double)), ("apply_launches", ctypes.POINTER(ctypes.c_int)),
                 ("apply_col_group", ctypes.c_int), ("apply_threads", ctypes.c_int),
-                ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int)]
+                ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int),
+                ("apply_tiles", ctypes.c_int)]
 
 
 _SIGS = {

@@ -17,6 +17,7 @@ int spmm_dispatch(const edx_csr* A, int k, int vec_type, const void* x, int64_t 
                   int64_t ycs, double2 al, double2 sg, double2 be, int kw, cudaStream_t st);
 int check_csr(const edx_csr* A);
 int auto_kw(int k);
+int pow2_kw(int k);
 
 constexpr int KT = 256;  // threads per block for the recurrence kernels
 
@@ -75,19 +76,25 @@ struct KrylovState {
 // b owns one contiguous range of rows).  Chunked keeps a block inside the contiguous row
 // ranges that share the high (bath) bits of the Fock states, where the impurity-internal
 // terms (Coulomb, spin-orbit, crystal field) land; their gathers then hit L1.
-template <int KW, class VT, int NT>
+template <int KW, int TG, class VT, int NT>
 __global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* __restrict__ row_ptr,
                                                       const int32_t* __restrict__ col, const VT* __restrict__ val,
                                                       const double2* __restrict__ Vc, double2* __restrict__ Vp,
                                                       KrylovState S, int it, int chunked) {
     constexpr int NW = NT / 32;
+    constexpr int BC = TG * KW;  // columns handled by this block
+    __shared__ double sh[NW * BC];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c = lane % KW;
     const int k = S.k;
-    const int gc = blockIdx.y * KW + c;
-    const bool colok = gc < k;
-    const double bprev = (colok && it > 0) ? S.beta[gc] : 0.0;
-    double apart = 0.0;
+    const int col0 = blockIdx.y * BC;
+    double bprev[TG], apart[TG];
+#pragma unroll
+    for (int g = 0; g < TG; ++g) {
+        const int gc = col0 + g * KW + c;
+        bprev[g] = (gc < k && it > 0) ? S.beta[gc] : 0.0;
+        apart[g] = 0.0;
+    }
     int64_t r0, r1, rstep;
     if (chunked) {
         const int64_t per = (n + gridDim.x - 1) / gridDim.x;
@@ -101,19 +108,37 @@ __global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* 
     }
     for (int64_t r = r0; r < r1; r += rstep) {
         const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
-        double2 acc = row_times_x<KW, VT, double2>(s, e, col, val, Vc, k, gc, colok);
-        if (lane < KW && colok) {
-            const int64_t o = r * k + gc;
-            double2 vp = Vp[o];
-            double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
-            w.x = w.x + acc.x;
-            w.y = w.y + acc.y;
-            Vp[o] = w;
-            double2 vc = Vc[o];
-            apart += vc.x * w.x + vc.y * w.y;  // Re(conj(v) w)
+        double2 acc[TG];
+        row_times_x_tiles<KW, TG, VT, double2>(s, e, col, val, Vc, k, col0, k, acc);
+        if (lane < KW) {
+#pragma unroll
+            for (int g = 0; g < TG; ++g) {
+                const int gc = col0 + g * KW + c;
+                if (gc < k) {
+                    const int64_t o = r * k + gc;
+                    double2 vp = Vp[o];
+                    double2 w = make_double2(-bprev[g] * vp.x, -bprev[g] * vp.y);
+                    w.x = w.x + acc[g].x;
+                    w.y = w.y + acc[g].y;
+                    Vp[o] = w;
+                    double2 vc = Vc[o];
+                    apart[g] += vc.x * w.x + vc.y * w.y;  // Re(conj(v) w)
+                }
+            }
         }
     }
-    block_col_partial<KW, NT>(apart, lane < KW, warp, NW, c, k, S.part);
+    // per-block column partials: sh[warp][g*KW + c], summed over warps in order
+    if (lane < KW) {
+#pragma unroll
+        for (int g = 0; g < TG; ++g) sh[warp * BC + g * KW + lane] = apart[g];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < BC; i += NT) {
+        double s = 0.0;
+        for (int w = 0; w < NW; ++w) s += sh[w * BC + i];
+        if (col0 + i < k) S.part[(int64_t)blockIdx.x * k + col0 + i] = s;
+    }
+    __syncthreads();
     if (arrive_last(S.ticket)) {
         for (int j = threadIdx.x; j < k; j += NT) {
             double a = sum_partials(S.part, gridDim.x, k, j);
@@ -318,34 +343,43 @@ __global__ void k_shift_final(int nshift, const ShiftState* __restrict__ st, int
 // launch shape of the fused apply kernel (chosen by the caller's autotuner, or defaults)
 struct ApplyCfg {
     int kw;         // columns per lane group
-    int threads;    // 256, 512 or 1024
+    int tg;         // column tiles per block (1, 2, 4; >1 only for kw 16 / 32)
+    int threads;    // 256 or 1024
     int gx;         // blocks along the rows
     int chunked;    // contiguous row ranges per block
 };
 
-template <int KW, class VT, int NT>
+template <int KW, int TG, class VT, int NT>
 static int launch_apply_nt(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
                            const ApplyCfg& cfg, cudaStream_t st) {
-    auto kern = k_lanczos_apply<KW, VT, NT>;
+    auto kern = k_lanczos_apply<KW, TG, VT, NT>;
     static bool carve_set = false;  // prefer L1 over shared memory: gathers are served from L1
     if (!carve_set) {
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
         carve_set = true;
     }
-    dim3 grid(cfg.gx, (S.k + KW - 1) / KW);
+    const int ntiles = (S.k + KW - 1) / KW;
+    dim3 grid(cfg.gx, (ntiles + TG - 1) / TG);
     kern<<<grid, NT, 0, st>>>(A->nrows, A->row_ptr, A->col, reinterpret_cast<const VT*>(A->val), Vc, Vp, S, it,
                               cfg.chunked);
     EDX_CHECK_LAUNCH();
     return EDX_OK;
 }
 
-template <int KW, class VT>
+template <int KW, int TG, class VT>
 static int launch_apply(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
                         const ApplyCfg& cfg, cudaStream_t st) {
-    switch (cfg.threads) {
-    case 512: return launch_apply_nt<KW, VT, 512>(A, Vc, Vp, S, it, cfg, st);
-    case 1024: return launch_apply_nt<KW, VT, 1024>(A, Vc, Vp, S, it, cfg, st);
-    default: return launch_apply_nt<KW, VT, 256>(A, Vc, Vp, S, it, cfg, st);
+    if (cfg.threads == 1024) return launch_apply_nt<KW, TG, VT, 1024>(A, Vc, Vp, S, it, cfg, st);
+    return launch_apply_nt<KW, TG, VT, 256>(A, Vc, Vp, S, it, cfg, st);
+}
+
+template <int KW, class VT>
+static int launch_apply_tg(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+                           const ApplyCfg& cfg, cudaStream_t st) {
+    switch (cfg.tg) {
+    case 2: return launch_apply<KW, 2, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 4: return launch_apply<KW, 4, VT>(A, Vc, Vp, S, it, cfg, st);
+    default: return launch_apply<KW, 1, VT>(A, Vc, Vp, S, it, cfg, st);
     }
 }
 
@@ -353,12 +387,14 @@ template <class VT>
 static int apply_v(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
                    const ApplyCfg& cfg, cudaStream_t st) {
     switch (cfg.kw) {
-    case 1: return launch_apply<1, VT>(A, Vc, Vp, S, it, cfg, st);
-    case 2: return launch_apply<2, VT>(A, Vc, Vp, S, it, cfg, st);
-    case 4: return launch_apply<4, VT>(A, Vc, Vp, S, it, cfg, st);
-    case 8: return launch_apply<8, VT>(A, Vc, Vp, S, it, cfg, st);
-    case 16: return launch_apply<16, VT>(A, Vc, Vp, S, it, cfg, st);
-    case 32: return launch_apply<32, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 1: return launch_apply<1, 1, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 2: return launch_apply<2, 1, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 4: return launch_apply<4, 1, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 6: return launch_apply<6, 1, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 8: return launch_apply<8, 1, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 12: return launch_apply<12, 1, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 16: return launch_apply_tg<16, VT>(A, Vc, Vp, S, it, cfg, st);
+    case 32: return launch_apply_tg<32, VT>(A, Vc, Vp, S, it, cfg, st);
     }
     return fail(EDX_ERR_INVALID, "krylov: bad column group %d", cfg.kw);
 }
@@ -462,16 +498,20 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     const int64_t n = A->nrows;
     ApplyCfg cfg;
     cfg.kw = (opts && opts->apply_col_group > 0) ? opts->apply_col_group : auto_kw(k);
-    cfg.threads = (opts && opts->apply_threads > 0) ? opts->apply_threads : 256;
-    const int bps = (opts && opts->apply_blocks_per_sm > 0) ? opts->apply_blocks_per_sm : 4;
+    cfg.threads = (opts && opts->apply_threads > 0) ? opts->apply_threads : 1024;
+    const int bps = (opts && opts->apply_blocks_per_sm > 0) ? opts->apply_blocks_per_sm : 1;
     cfg.chunked = (opts && opts->apply_chunked > 0) ? 1 : 0;
-    EDX_REQUIRE(cfg.kw == 1 || cfg.kw == 2 || cfg.kw == 4 || cfg.kw == 8 || cfg.kw == 16 || cfg.kw == 32,
-                "edx_krylov: apply_col_group must be a power of two <= 32");
-    EDX_REQUIRE(cfg.threads == 256 || cfg.threads == 512 || cfg.threads == 1024,
-                "edx_krylov: apply_threads must be 256, 512 or 1024");
+    const int ntiles = (k + cfg.kw - 1) / cfg.kw;
+    cfg.tg = (opts && opts->apply_tiles > 0) ? opts->apply_tiles : (ntiles >= 4 ? 4 : (ntiles >= 2 ? 2 : 1));
+    if (cfg.kw < 16) cfg.tg = 1;
+    EDX_REQUIRE(cfg.kw == 1 || cfg.kw == 2 || cfg.kw == 4 || cfg.kw == 6 || cfg.kw == 8 || cfg.kw == 12 ||
+                    cfg.kw == 16 || cfg.kw == 32,
+                "edx_krylov: apply_col_group must be one of 1, 2, 4, 6, 8, 12, 16, 32");
+    EDX_REQUIRE(cfg.tg == 1 || cfg.tg == 2 || cfg.tg == 4, "edx_krylov: apply_tiles must be 1, 2 or 4");
+    EDX_REQUIRE(cfg.threads == 256 || cfg.threads == 1024, "edx_krylov: apply_threads must be 256 or 1024");
     EDX_REQUIRE(bps >= 1 && bps * cfg.threads <= 8 * 256, "edx_krylov: apply_blocks_per_sm out of range");
     cfg.gx = num_sms() * bps;
-    const int kw = cfg.kw;
+    const int kw = pow2_kw(k);  // layout of the element-wise recurrence kernels
     const int gy = (k + kw - 1) / kw;
     const int gx = num_sms() * 8;
     Workspace w(d_work, work_bytes);

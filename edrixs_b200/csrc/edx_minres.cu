@@ -70,7 +70,9 @@ __global__ void __launch_bounds__(MT) k_mr_apply(int64_t n, const int64_t* __res
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t r = w0; r < n; r += nw) {
         const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
-        double2 acc = row_times_x<1, VT, double2>(s, e, col, val, v, 1, 0, true);
+        double2 accv[1];
+        row_times_x_tiles<1, 1, VT, double2>(s, e, col, val, v, 1, 0, 1, accv);
+        const double2 acc = accv[0];
         if (lane == 0) {
             double2 vr = v[r];
             double2 t = cmul(aop, acc);

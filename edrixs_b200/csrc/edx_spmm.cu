@@ -26,7 +26,9 @@ __global__ void __launch_bounds__(256) k_spmm(int64_t nrows, const int64_t* __re
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t r = warp0; r < nrows; r += nw) {
         const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
-        AT acc = row_times_x<KW, VT, XT>(s, e, col, val, X, ldx_, gc, colok);
+        AT accv[1];
+        row_times_x_tiles<KW, 1, VT, XT>(s, e, col, val, X, ldx_, blockIdx.y * KW, k, accv);
+        const AT acc = accv[0];
         if (lane < KW && colok) {
             double yr = alpha.x * (double)acc.x - alpha.y * (double)acc.y;
             double yi = alpha.x * (double)acc.y + alpha.y * (double)acc.x;
@@ -75,14 +77,25 @@ static int launch_spmm_v(const edx_csr* A, int k, int kw, const void* x, int64_t
     case 1: return launch_spmm_t<1, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
     case 2: return launch_spmm_t<2, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
     case 4: return launch_spmm_t<4, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    case 6: return launch_spmm_t<6, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
     case 8: return launch_spmm_t<8, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    case 12: return launch_spmm_t<12, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
     case 16: return launch_spmm_t<16, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
     case 32: return launch_spmm_t<32, VT, XT>(A, k, x, ldx_, y, ldy, ycs, al, sg, be, st);
     }
     return fail(EDX_ERR_INVALID, "spmm: unsupported column group width %d", kw);
 }
 
+// columns per lane group: the smallest supported width >= k (k <= 32), else 32 with tiles
 int auto_kw(int k) {
+    static const int widths[] = {1, 2, 4, 6, 8, 12, 16, 32};
+    for (int w : widths)
+        if (w >= k) return w;
+    return 32;
+}
+
+// power-of-two width for the element-wise recurrence kernels
+int pow2_kw(int k) {
     int kw = 1;
     while (kw < k && kw < 32) kw <<= 1;
     return kw;
@@ -123,9 +136,9 @@ extern "C" int edx_spmm(const edx_csr* A, int k, int vec_type, const void* d_x, 
     EDX_REQUIRE(vec_type == EDX_C128 || vec_type == EDX_C64, "edx_spmm: bad vec_type");
     if ((sigma_re != 0.0 || sigma_im != 0.0))
         EDX_REQUIRE(A->nrows == A->ncols, "edx_spmm: sigma needs a square matrix");
-    EDX_REQUIRE(col_group == 0 || col_group == 1 || col_group == 2 || col_group == 4 ||
-                    col_group == 8 || col_group == 16 || col_group == 32,
-                "edx_spmm: column group width must be a power of two <= 32");
+    EDX_REQUIRE(col_group == 0 || col_group == 1 || col_group == 2 || col_group == 4 || col_group == 6 ||
+                    col_group == 8 || col_group == 12 || col_group == 16 || col_group == 32,
+                "edx_spmm: column group width must be one of 1, 2, 4, 6, 8, 12, 16, 32");
     if (A->nrows == 0) return EDX_OK;
     return spmm_dispatch(A, k, vec_type, d_x, ldx_, d_y, ldy, 1, make_double2(alpha_re, alpha_im),
                          make_double2(sigma_re, sigma_im), make_double2(beta_re, beta_im), col_group,

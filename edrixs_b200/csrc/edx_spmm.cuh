@@ -55,27 +55,68 @@ __device__ __forceinline__ float2 zero_c<float2>() { return make_float2(0.f, 0.f
 __device__ __forceinline__ double2 ldx(const double2* p) { return __ldg(p); }
 __device__ __forceinline__ float2 ldx(const float2* p) { return __ldg(p); }
 
-// Row r times column gc of X for a warp where lane = slot * KW + c (SLOTS = 32 / KW):
-// the warp streams the row's nonzeros in chunks of 32 (one coalesced load per lane), then
-// each slot takes every SLOTS-th entry of the chunk by shuffle.  Returns the full row sum in
-// every lane of column c (slots reduced by xor-shuffles).
-template <int KW, class VT, class XT>
-__device__ __forceinline__ typename Acc<VT, XT>::T row_times_x(int64_t start, int64_t end,
-                                                               const int32_t* __restrict__ col,
-                                                               const VT* __restrict__ val,
-                                                               const XT* __restrict__ X, int64_t ldx_,
-                                                               int gc, bool colok) {
+// Lane layout of a warp working on one row: lane = slot * KW + c with SLOTS = 32 / KW slots
+// (KW need not be a power of two; lanes beyond SLOTS*KW idle).  The warp streams the row's
+// nonzeros in chunks of 32 (one coalesced load per lane); each slot takes every SLOTS-th
+// entry of a chunk by shuffle.  This product is bound by gather latency, so the loops below
+// issue several independent gathers before consuming any of them.
+template <int KW>
+struct Slots {
+    static constexpr int N = 32 / KW;
+    static constexpr bool POW2 = (KW & (KW - 1)) == 0;
+};
+
+// Row r times TG column tiles of X (columns (tile0 + g)*KW + c, g < TG) with explicit
+// memory-level parallelism: per chunk of 32 nonzeros, U entries per slot are shuffled out
+// first, then all U*TG gathers are issued, then the FMAs run.  acc[g] holds the row sum of
+// tile g in every lane of column c on return.  Lanes with slot >= SLOTS idle.
+template <int KW, int TG, class VT, class XT>
+__device__ __forceinline__ void row_times_x_tiles(int64_t start, int64_t end, const int32_t* __restrict__ col,
+                                                  const VT* __restrict__ val, const XT* __restrict__ X,
+                                                  int64_t ldx_, int col0, int k, typename Acc<VT, XT>::T* acc) {
     using AT = typename Acc<VT, XT>::T;
-    constexpr int SLOTS = 32 / KW;
+    constexpr int SLOTS = Slots<KW>::N;
+    constexpr int GROUPS = (32 + SLOTS - 1) / SLOTS;          // entry groups per chunk
+    constexpr int U0 = (8 / TG) > 0 ? (8 / TG) : 1;           // gathers in flight per lane ~ 8
+    constexpr int U = U0 < GROUPS ? U0 : GROUPS;
     const int lane = threadIdx.x & 31;
     const int slot = lane / KW;
-    AT acc = zero_c<AT>();
+    const int c = lane % KW;
+    const bool slot_ok = slot < SLOTS;
+    bool colok[TG];
+#pragma unroll
+    for (int g = 0; g < TG; ++g) {
+        colok[g] = slot_ok && (col0 + g * KW + c < k);
+        acc[g] = zero_c<AT>();
+    }
     if (KW == 1) {
-        for (int64_t j = start + lane; j < end; j += 32) {
-            int c = ld_stream(col + j);
-            AT v = to_acc(ld_stream(val + j), AT());
-            AT x = to_acc(ldx(X + (int64_t)c * ldx_ + gc), AT());
-            acc = fma_c(v, x, acc);
+        // each lane owns its own entries; U rounds of 32 per pass
+        for (int64_t base = start; base < end; base += 32 * U) {
+            int cc[U];
+            AT vv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t j = base + u * 32 + lane;
+                cc[u] = 0;
+                vv[u] = zero_c<AT>();
+                if (j < end) {
+                    cc[u] = ld_stream(col + j);
+                    vv[u] = to_acc(ld_stream(val + j), AT());
+                }
+            }
+            AT xs[U][TG];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int g = 0; g < TG; ++g) {
+                    xs[u][g] = zero_c<AT>();
+                    if (base + u * 32 + lane < end && colok[g])
+                        xs[u][g] = to_acc(ldx(X + (int64_t)cc[u] * ldx_ + col0 + g), AT());
+                }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int g = 0; g < TG; ++g) acc[g] = fma_c(vv[u], xs[u][g], acc[g]);
         }
     } else {
         for (int64_t base = start; base < end; base += 32) {
@@ -89,22 +130,52 @@ __device__ __forceinline__ typename Acc<VT, XT>::T row_times_x(int64_t start, in
                 vj = ld_stream(val + j);
             }
             const int cnt = (end - base < 32) ? (int)(end - base) : 32;
-#pragma unroll 4
-            for (int t = 0; t < 32; t += SLOTS) {
-                if (t >= cnt) break;
-                const int src = t + slot;
-                const int cc = __shfl_sync(0xffffffffu, cj, src);
-                const VT vv = shfl2(vj, src);
-                if (src < cnt && colok) {
-                    AT x = to_acc(ldx(X + (int64_t)cc * ldx_ + gc), AT());
-                    acc = fma_c(to_acc(vv, AT()), x, acc);
+#pragma unroll
+            for (int q0 = 0; q0 < GROUPS; q0 += U) {
+                int cc[U];
+                AT vv[U];
+                bool ok[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int src = (q0 + u) * SLOTS + slot;
+                    cc[u] = __shfl_sync(0xffffffffu, cj, src & 31);
+                    VT t = shfl2(vj, src & 31);
+                    vv[u] = to_acc(t, AT());
+                    ok[u] = (q0 + u < GROUPS) && src < cnt;
                 }
+                AT xs[U][TG];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int g = 0; g < TG; ++g) {
+                        xs[u][g] = zero_c<AT>();
+                        if (ok[u] && colok[g])
+                            xs[u][g] = to_acc(ldx(X + (int64_t)cc[u] * ldx_ + col0 + g * KW + c), AT());
+                    }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int g = 0; g < TG; ++g) acc[g] = fma_c(vv[u], xs[u][g], acc[g]);
             }
         }
     }
 #pragma unroll
-    for (int off = KW; off < 32; off <<= 1) acc = xor_sum(acc, off);
-    return acc;
+    for (int g = 0; g < TG; ++g) {
+        if (Slots<KW>::POW2) {
+#pragma unroll
+            for (int off = KW; off < 32; off <<= 1) acc[g] = xor_sum(acc[g], off);
+        } else {
+            AT tot = zero_c<AT>();
+#pragma unroll
+            for (int s = 0; s < SLOTS; ++s) {
+                AT o;
+                o.x = __shfl_sync(0xffffffffu, acc[g].x, s * KW + c);
+                o.y = __shfl_sync(0xffffffffu, acc[g].y, s * KW + c);
+                tot = add_c(tot, o);
+            }
+            acc[g] = tot;
+        }
+    }
 }
 
 }  // namespace edx

@@ -13,13 +13,26 @@ _cache = {}
 
 
 def candidates(k):
-    kws = [0] if k <= 32 else [32, 16]
-    shapes = [(256, 4), (256, 8), (512, 2), (512, 4), (1024, 1), (1024, 2)]
+    if k > 32:
+        kws = [32, 16]
+    else:
+        # the smallest group width >= k, and the next power of two (fewer idle lanes vs
+        # simpler slot reduction)
+        widths = [1, 2, 4, 6, 8, 12, 16, 32]
+        first = next(w for w in widths if w >= k)
+        pow2 = next(w for w in (1, 2, 4, 8, 16, 32) if w >= k)
+        kws = sorted({first, pow2})
+    shapes = [(256, 4), (256, 8), (1024, 1), (1024, 2)]
     out = []
     for kw in kws:
-        for th, bps in shapes:
-            for ch in (0, 1):
-                out.append(dict(col_group=kw, threads=th, blocks_per_sm=bps, chunked=ch))
+        tiles = [1]
+        if kw >= 16:
+            nt = (k + kw - 1) // kw
+            tiles = [t for t in (1, 2, 4) if t <= nt]
+        for tg in tiles:
+            for th, bps in shapes:
+                for ch in (0, 1):
+                    out.append(dict(col_group=kw, tiles=tg, threads=th, blocks_per_sm=bps, chunked=ch))
     return out
 
 

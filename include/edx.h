@@ -163,12 +163,14 @@ typedef struct edx_krylov_opts {
     double* apply_ms;
     int* apply_launches;
     /* launch shape of the fused SpMM + recurrence kernel (0 = default): columns per lane
-     * group (power of two <= 32), threads per block (256/512/1024), blocks per SM, and the
-     * row mapping (0 = interleaved rows, 1 = one contiguous row range per block) */
+     * group (1, 2, 4, 6, 8, 12, 16 or 32), threads per block (256 or 1024), blocks per SM,
+     * row mapping (0 = interleaved rows, 1 = one contiguous row range per block), and
+     * column tiles per block (1, 2 or 4; group widths 16 and 32 only) */
     int apply_col_group;
     int apply_threads;
     int apply_blocks_per_sm;
     int apply_chunked;
+    int apply_tiles;
 } edx_krylov_opts;
 
 /* k independent Lanczos recurrences of build_krylov_mp (src/lanczos.f90:210-303), run

@@ -211,6 +211,69 @@ def cpu_sample(args, t, gs, omega, iters_minres, minres_its=60, krylov_steps=60)
 # arms
 # ------------------------------------------------------------------------------------
 
+def accuracy_report(P, res, plain, omegas, eloss, w_idx, nkryl, npin=2, npout=2, ngs=3):
+    """Batched vs the plain FP64 one-RHS path at one incident energy, next to the conditioning
+    floor of the reference's final-state Lanczos (150 steps, no reorthogonalisation): the
+    change of the plain path's own spectrum when its start vector moves by 1e-14 relative."""
+    import torch
+    from edrixs_b200 import device, rixs
+    n_om = len(omegas)
+    k = npin * ngs
+    w = rixs.boltz(P.gs_e, 300.0)
+
+    def spectrum(sets, gamma):
+        A = torch.stack([s[0] for s in sets])
+        B = torch.stack([s[1] for s in sets])
+        NR = np.array([s[2] for s in sets])
+        NE = torch.tensor([s[3] for s in sets], dtype=torch.int32, device="cuda")
+        return device.cf_spectrum(NE, A, B, P.gs_e, NR, w, eloss, np.full(len(eloss), gamma)).cpu().numpy()
+
+    def batched_set(pi, po, g):
+        j = (po * k + pi * ngs + g) * n_om + w_idx
+        pl = res.poles
+        return pl["alpha"][j], pl["beta"][j], float(pl["norm"][j]), int(pl["neff"][j])
+
+    def plain_set(pi, po, g):
+        rf = plain[(pi, po, g)]
+        return rf.alpha[0], rf.beta[0], float(rf.norm[0]), int(rf.neff[0])
+
+    def perturbed_set(pi, po, g, eps, gen):
+        b = device.spmm(P.Din[pi], P.gs_v[:, g].contiguous())
+        z = complex(omegas[w_idx] + P.gs_e[g], 0.6)
+        x, _, _ = device.minres(P.Hn, b, 1e-10, 1000, alpha=-1.0, sigma=z)
+        phi = device.spmm(P.Dout[po], x)
+        noise = torch.randn(phi.shape, dtype=torch.float64, device="cuda", generator=gen)
+        rf = device.krylov(P.Hf, (phi * (1 + eps * noise)).reshape(-1, 1), nkryl)
+        return rf.alpha[0], rf.beta[0], float(rf.norm[0]), int(rf.neff[0])
+
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    out = {"omega_index": int(w_idx), "spectra_rel_err": {}, "conditioning_floor": {"perturbation": 1e-14}}
+    pert = {(pi, po): [perturbed_set(pi, po, g, 1e-14, gen) for g in range(ngs)] for pi in range(npin)
+            for po in range(npout)}
+    for gamma in (0.1, 1.0):
+        err = floor = 0.0
+        for pi in range(npin):
+            for po in range(npout):
+                sp = spectrum([plain_set(pi, po, g) for g in range(ngs)], gamma)
+                sb = spectrum([batched_set(pi, po, g) for g in range(ngs)], gamma)
+                sq = spectrum(pert[(pi, po)], gamma)
+                scale = np.abs(sp).max()
+                err = max(err, float(np.abs(sb - sp).max() / scale))
+                floor = max(floor, float(np.abs(sq - sp).max() / scale))
+        out["spectra_rel_err"][f"gamma_f_{gamma}"] = err
+        out["conditioning_floor"][f"gamma_f_{gamma}"] = floor
+    # the first Lanczos coefficients, before orthogonality is lost, are well conditioned
+    d = 0.0
+    for key in plain:
+        a_p, b_p = plain_set(*key)[:2]
+        a_b, b_b = batched_set(*key)[:2]
+        d = max(d, float((a_b[:10] - a_p[:10]).abs().max() / a_p[:10].abs().max()),
+                float((b_b[:10] - b_p[:10]).abs().max() / b_p[:10].abs().max()))
+    out["lanczos_first10_rel_err"] = d
+    return out
+
+
 def run_ours(args):
     import torch
     from edrixs_b200 import dist, rixs
@@ -234,6 +297,7 @@ def run_ours(args):
         barrier()
         torch.cuda.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed")  # lets a profiler select exactly the timed steps
         ev0.record()
         for _ in range(args.steps):
             s0 = torch.cuda.Event(enable_timing=True)
@@ -244,6 +308,7 @@ def run_ours(args):
             stats.append(res.stats)
             lat.append((s0, s1))
         ev1.record()
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         barrier()
     total_ms = ev0.elapsed_time(ev1)
@@ -293,30 +358,19 @@ def run_ours(args):
         torch.cuda.synchronize()
         w_idx = n_om // 2
         p0 = time.perf_counter()
-        spec_plain = np.zeros((len(eloss), 4))
-        from edrixs_b200 import device
+        plain = {}
         for pi in range(2):
             for po in range(2):
-                sets = []
                 for g in range(3):
-                    rf, it, rr = rixs.rixs_plain(P, omegas[w_idx], 0.6, eloss, 0.1, pin=pi, pout=po, g=g,
-                                                 nkryl=args.nkryl, linsys_tol=1e-10, linsys_max=1000)
-                    sets.append(rf)
-                A = torch.cat([s.alpha for s in sets])
-                B = torch.cat([s.beta for s in sets])
-                NR = torch.cat([s.norm for s in sets])
-                NE = torch.cat([s.neff for s in sets])
-                spec_plain[:, pi * 2 + po] = device.cf_spectrum(
-                    NE, A, B, P.gs_e, NR.cpu().numpy(), rixs.boltz(P.gs_e, 300.0), eloss,
-                    np.full(len(eloss), 0.1)).cpu().numpy()
+                    plain[(pi, po, g)] = rixs.rixs_plain(P, omegas[w_idx], 0.6, eloss, 0.1, pin=pi, pout=po, g=g,
+                                                         nkryl=args.nkryl, linsys_tol=1e-10, linsys_max=1000)[0]
         torch.cuda.synchronize()
         plain_s = time.perf_counter() - p0
-        batched = res.spectra[w_idx]
-        err = float(np.abs(batched - spec_plain).max() / np.abs(spec_plain).max())
         extra["plain_fp64_one_rhs"] = {"seconds_per_omega_in": round(plain_s, 3),
                                        "value": round(1.0 / plain_s, 4), "unit": UNIT,
                                        "batched_over_plain": round(value / ws / (1.0 / plain_s), 2)}
-        extra["rel_err_vs_fp64_plain"] = err
+        extra["accuracy"] = accuracy_report(P, res, plain, omegas, eloss, w_idx, args.nkryl)
+        extra["rel_err_vs_fp64_plain"] = extra["accuracy"]["spectra_rel_err"]["gamma_f_0.1"]
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

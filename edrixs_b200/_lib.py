@@ -49,7 +49,7 @@ class KrylovOpts(ctypes.Structure):
                 ("apply_ms", ctypes.POINTER(ctypes.c_double)), ("apply_launches", ctypes.POINTER(ctypes.c_int)),
                 ("apply_col_group", ctypes.c_int), ("apply_threads", ctypes.c_int),
                 ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int),
-                ("apply_tiles", ctypes.c_int)]
+                ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int)]
 
 
 _SIGS = {

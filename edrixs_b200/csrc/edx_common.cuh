@@ -144,6 +144,23 @@ __device__ __forceinline__ float2 ld_stream(const float2* p) {
                  : "l"(p), "l"(evict_first_policy()));
     return v;
 }
+// TMA bulk prefetch of bytes [begin, end) of `base` into L2.  The untiled bulk form needs a
+// 16-byte aligned address and a size that is a multiple of 16: the range is widened to 16-byte
+// boundaries and clamped to the last full 16-byte block below `limit` (the array's byte size),
+// so it never reaches past the array.  A prefetch is a hint; nothing waits on it.
+__device__ __forceinline__ void prefetch_l2(const void* base, int64_t begin, int64_t end, int64_t limit) {
+    int64_t a0 = begin & ~int64_t(15);
+    int64_t a1 = (end + 15) & ~int64_t(15);
+    const int64_t lim = limit & ~int64_t(15);
+    if (a1 > lim) a1 = lim;
+    if (a1 <= a0) return;
+    int64_t size = a1 - a0;
+    if (size > (int64_t)1 << 20) size = (int64_t)1 << 20;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(static_cast<const char*>(base) + a0),
+                 "r"((unsigned)size)
+                 : "memory");
+}
+
 __device__ __forceinline__ int ld_stream(const int* p) {
     int v;
     asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"

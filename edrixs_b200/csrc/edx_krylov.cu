@@ -80,9 +80,10 @@ template <int KW, int TG, class VT, int NT>
 __global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* __restrict__ row_ptr,
                                                       const int32_t* __restrict__ col, const VT* __restrict__ val,
                                                       const double2* __restrict__ Vc, double2* __restrict__ Vp,
-                                                      KrylovState S, int it, int chunked) {
+                                                      KrylovState S, int it, int chunked, int prefetch) {
     constexpr int NW = NT / 32;
     constexpr int BC = TG * KW;  // columns handled by this block
+    const int64_t nnz = prefetch ? __ldg(row_ptr + n) : 0;
     __shared__ double sh[NW * BC];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int c = lane % KW;
@@ -108,6 +109,12 @@ __global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* 
     }
     for (int64_t r = r0; r < r1; r += rstep) {
         const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
+        if (prefetch && lane == 0 && r + rstep < r1) {
+            // bring this warp's next row (indices and values) into L2 while this one runs
+            const int64_t sn = __ldg(row_ptr + r + rstep), en = __ldg(row_ptr + r + rstep + 1);
+            prefetch_l2(col, sn * 4, en * 4, nnz * 4);
+            prefetch_l2(val, sn * (int64_t)sizeof(VT), en * (int64_t)sizeof(VT), nnz * (int64_t)sizeof(VT));
+        }
         double2 acc[TG];
         row_times_x_tiles<KW, TG, VT, double2>(s, e, col, val, Vc, k, col0, k, acc);
         if (lane < KW) {
@@ -347,6 +354,7 @@ struct ApplyCfg {
     int threads;    // 256 or 1024
     int gx;         // blocks along the rows
     int chunked;    // contiguous row ranges per block
+    int prefetch;   // bulk-prefetch each warp's next row into L2
 };
 
 template <int KW, int TG, class VT, int NT>
@@ -361,7 +369,7 @@ static int launch_apply_nt(const edx_csr* A, const double2* Vc, double2* Vp, con
     const int ntiles = (S.k + KW - 1) / KW;
     dim3 grid(cfg.gx, (ntiles + TG - 1) / TG);
     kern<<<grid, NT, 0, st>>>(A->nrows, A->row_ptr, A->col, reinterpret_cast<const VT*>(A->val), Vc, Vp, S, it,
-                              cfg.chunked);
+                              cfg.chunked, cfg.prefetch);
     EDX_CHECK_LAUNCH();
     return EDX_OK;
 }
@@ -501,6 +509,7 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     cfg.threads = (opts && opts->apply_threads > 0) ? opts->apply_threads : 1024;
     const int bps = (opts && opts->apply_blocks_per_sm > 0) ? opts->apply_blocks_per_sm : 1;
     cfg.chunked = (opts && opts->apply_chunked > 0) ? 1 : 0;
+    cfg.prefetch = (opts && opts->apply_prefetch > 0) ? 1 : 0;
     const int ntiles = (k + cfg.kw - 1) / cfg.kw;
     cfg.tg = (opts && opts->apply_tiles > 0) ? opts->apply_tiles : (ntiles >= 4 ? 4 : (ntiles >= 2 ? 2 : 1));
     if (cfg.kw < 16) cfg.tg = 1;

@@ -403,3 +403,4 @@ extern "C" int edx_denmat(const uint64_t* d_fock, int64_t n, int search_norb, in
     EDX_CHECK_LAUNCH();
     return EDX_OK;
 }
+

@@ -254,6 +254,7 @@ def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, s
         opts.apply_blocks_per_sm = int(apply.get("blocks_per_sm", 0))
         opts.apply_chunked = int(apply.get("chunked", 0))
         opts.apply_tiles = int(apply.get("tiles", 0))
+        opts.apply_prefetch = int(apply.get("prefetch", 0))
     ms = ctypes.c_double(0.0)
     nl = ctypes.c_int(0)
     if timing:

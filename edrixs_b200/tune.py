@@ -32,7 +32,9 @@ def candidates(k):
         for tg in tiles:
             for th, bps in shapes:
                 for ch in (0, 1):
-                    out.append(dict(col_group=kw, tiles=tg, threads=th, blocks_per_sm=bps, chunked=ch))
+                    for pf in (0, 1):
+                        out.append(dict(col_group=kw, tiles=tg, threads=th, blocks_per_sm=bps, chunked=ch,
+                                        prefetch=pf))
     return out
 
 

@@ -124,7 +124,8 @@ typedef struct edx_csr {
  * With beta = 1, sigma = 0 this is matvec_csr's y += A x (src/spmv.f90:73-103, the
  * per-rank kernel of pspmv_csr src/spmv.f90:1-71).  vec_type: EDX_C128 or EDX_C64 for X
  * and Y; C64 X/Y require a C64 matrix (complex64 arithmetic).  col_group: columns handled
- * per lane group of a warp (power of two <= 32; 0 = smallest power of two >= min(k, 32)). */
+ * per lane group of a warp (1, 2, 4, 6, 8, 12, 16 or 32; 0 = the smallest of those >= k,
+ * capped at 32 with column tiles beyond). */
 int edx_spmm(const edx_csr* A, int k, int vec_type, const void* d_x, int64_t ldx, void* d_y,
              int64_t ldy, double alpha_re, double alpha_im, double sigma_re, double sigma_im,
              double beta_re, double beta_im, int col_group, void* stream);
@@ -165,12 +166,14 @@ typedef struct edx_krylov_opts {
     /* launch shape of the fused SpMM + recurrence kernel (0 = default): columns per lane
      * group (1, 2, 4, 6, 8, 12, 16 or 32), threads per block (256 or 1024), blocks per SM,
      * row mapping (0 = interleaved rows, 1 = one contiguous row range per block), and
-     * column tiles per block (1, 2 or 4; group widths 16 and 32 only) */
+     * column tiles per block (1, 2 or 4; group widths 16 and 32 only), and whether each
+     * warp bulk-prefetches its next row into L2 (cp.async.bulk.prefetch) */
     int apply_col_group;
     int apply_threads;
     int apply_blocks_per_sm;
     int apply_chunked;
     int apply_tiles;
+    int apply_prefetch;
 } edx_krylov_opts;
 
 /* k independent Lanczos recurrences of build_krylov_mp (src/lanczos.f90:210-303), run
@@ -212,6 +215,7 @@ int edx_denmat_workspace(int64_t n, int nv, int nvec, size_t* bytes);
 int edx_denmat(const uint64_t* d_fock, int64_t n, int search_norb, int search_nelec, int nv,
                int nvec, const double* d_vecs, double* d_out, void* d_work, size_t work_bytes,
                void* stream);
+
 
 #ifdef __cplusplus
 }

@@ -83,6 +83,8 @@ _SIGS = {
     "edx_denmat_workspace": (ctypes.c_int, [i64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "edx_denmat": (ctypes.c_int, [vp, i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp,
                                   ctypes.c_size_t, vp]),
+    "edx_denmat_static": (ctypes.c_int, [vp, i64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp,
+                                         vp]),
 }
 
 _lib = None

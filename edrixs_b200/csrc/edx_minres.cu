@@ -1,6 +1,7 @@
 // edx_minres.cu -- one-RHS MINRES (K12, plain FP64 path), continued fraction (K13) and
 // density matrix (K14).
 #include <algorithm>
+#include <mutex>
 
 #include "edx_fock.cuh"
 #include "edx_spmm.cuh"
@@ -404,3 +405,66 @@ extern "C" int edx_denmat(const uint64_t* d_fock, int64_t n, int search_norb, in
     return EDX_OK;
 }
 
+// ---- density matrix with no allocation at all ---------------------------------------------
+// Some hosts cannot give this library device memory: a host whose HBM is fully carved up
+// by its own allocator before the solve (a serving process that has reserved its whole
+// budget for resident Hamiltonians), or a thin foreign-language binding that only forwards
+// the eigenvector buffers it was handed and has no CUDA allocator to make a workspace.
+// edx_denmat_static keeps the per-chunk partial sums of k_denmat in a fixed array in the
+// library's own device memory instead.
+namespace edx {
+
+static __device__ __align__(256) double2
+    g_denmat_scratch[(size_t)EDX_DENMAT_STATIC_CHUNKS * EDX_DENMAT_STATIC_MAX_ENTRIES];
+
+static std::mutex g_denmat_scratch_mu;
+static double2* g_denmat_scratch_ptr[EDX_MAX_DEVICES];
+
+// Device address of g_denmat_scratch for the current device.  In host code the symbol's
+// name is only a host-side stand-in, so the address is looked up once per device, with that
+// device current, and cached.
+static int denmat_scratch_address(double2** out) {
+    int dev = 0;
+    EDX_CUDA(cudaGetDevice(&dev));
+    EDX_REQUIRE(dev >= 0 && dev < EDX_MAX_DEVICES, "edx_denmat_static: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_denmat_scratch_mu);
+    if (g_denmat_scratch_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_denmat_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            return fail(EDX_ERR_CUDA, "edx_denmat_static: cudaGetSymbolAddress of the scratch array failed: %s",
+                        cudaGetErrorString(e));
+        g_denmat_scratch_ptr[dev] = static_cast<double2*>(p);
+    }
+    *out = g_denmat_scratch_ptr[dev];
+    return EDX_OK;
+}
+
+}  // namespace edx
+
+extern "C" int edx_denmat_static(const uint64_t* d_fock, int64_t n, int search_norb, int search_nelec, int nv,
+                                 int nvec, const double* d_vecs, double* d_out, void* stream) {
+    EDX_REQUIRE(d_fock && d_vecs && d_out && n >= 1 && nvec >= 1, "edx_denmat_static: bad arguments");
+    EDX_REQUIRE(nv >= 1 && nv <= 63, "edx_denmat_static: nv must be 1..63");
+    const int64_t P = (int64_t)nvec * nv * nv;
+    EDX_REQUIRE(P <= EDX_DENMAT_STATIC_MAX_ENTRIES,
+                "edx_denmat_static: nvec*nv*nv = %lld exceeds the static scratch limit of %d entries "
+                "(use edx_denmat with a workspace)",
+                (long long)P, EDX_DENMAT_STATIC_MAX_ENTRIES);
+    double2* part = nullptr;
+    int rc = denmat_scratch_address(&part);
+    if (rc) return rc;
+    cudaStream_t st = as_stream(stream);
+    // every (chunk, entry) slot the sum below reads is written by this call's k_denmat, so
+    // nothing in the scratch array has to be cleared first
+    const int nch = std::min(denmat_chunks(n), EDX_DENMAT_STATIC_CHUNKS);
+    const int64_t rpc = (n + nch - 1) / nch;
+    dim3 grid(nch, (unsigned)((P + 255) / 256));
+    size_t smem = search_norb > 0 ? binom_bytes(search_norb, search_nelec) : 0;
+    k_denmat<<<grid, 256, smem, st>>>(d_fock, n, search_norb, search_nelec, nv, nvec,
+                                      reinterpret_cast<const double2*>(d_vecs), rpc, part);
+    EDX_CHECK_LAUNCH();
+    k_denmat_sum<<<(unsigned)((P + 255) / 256), 256, 0, st>>>(nch, (int)P, part, reinterpret_cast<double2*>(d_out));
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}

@@ -216,6 +216,22 @@ int edx_denmat(const uint64_t* d_fock, int64_t n, int search_norb, int search_ne
                int nvec, const double* d_vecs, double* d_out, void* d_work, size_t work_bytes,
                void* stream);
 
+/* The density matrix of edx_denmat for callers that cannot allocate device memory and so
+ * cannot pass a workspace (no counterpart in the reference, which allocates as it pleases).
+ * Examples: a host whose HBM is carved up in advance by its own allocator, or a thin
+ * foreign-language binding that only forwards buffers it was handed.  The partial sums live
+ * in a fixed file-scope device array of EDX_DENMAT_STATIC_CHUNKS x
+ * EDX_DENMAT_STATIC_MAX_ENTRIES complex128 values (4 MiB) that every GPU loading the library
+ * holds until the process exits.  Limit: nvec * nv * nv <= EDX_DENMAT_STATIC_MAX_ENTRIES,
+ * otherwise EDX_ERR_INVALID.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the GPU (for
+ * example on two streams) race and must be serialised by the caller.  Allocates nothing. */
+#define EDX_DENMAT_STATIC_CHUNKS 64
+#define EDX_DENMAT_STATIC_MAX_ENTRIES 4096
+#define EDX_MAX_DEVICES 64
+int edx_denmat_static(const uint64_t* d_fock, int64_t n, int search_norb, int search_nelec,
+                      int nv, int nvec, const double* d_vecs, double* d_out, void* stream);
 
 #ifdef __cplusplus
 }

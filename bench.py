@@ -44,15 +44,19 @@ def parse():
     ap.add_argument("--c64", action="store_true", help="complex64 matrices in the Krylov products")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--kernel-case", choices=["apply"], default=None,
+    ap.add_argument("--no-tiles", action="store_true", help="no tiled layout of H_f (CSR product only)")
+    ap.add_argument("--kernel-case", choices=["apply", "hf-shapes"], default=None,
                     help="run only a small profiling case of the dominant kernels (for ncu)")
     return ap.parse_args()
 
 
 def kernel_case(args):
-    """The apply kernels on this workload's matrices, two launches each (a few GB on the
-    device): H_n with the 6 seed columns, H_f with 256 final-state columns, and one SpMV of
-    the one-RHS MINRES.  Launch shapes are the autotuner's usual winners."""
+    """The apply kernels on this workload's matrices at the launch shapes the autotuner picks
+    for the timed steps (a few GB on the device): one Lanczos step of H_n on the 6 seed
+    columns, one of H_f on 256 final-state columns (each column group of 64 sweeps the same
+    rows and x columns as in the 768-column timed launches, one third as many groups), and
+    one SpMV of the one-RHS MINRES.  Each Krylov call of two steps launches the apply
+    kernel twice."""
     import torch
     from edrixs_b200 import device
     m, t = workload_terms(args.nbath, args.nelec)
@@ -63,13 +67,32 @@ def kernel_case(args):
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     V = torch.randn((Hn.nrows, 6), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
-    device.krylov(Hn, V, 2, apply=dict(threads=1024, blocks_per_sm=1, chunked=1))
+    device.krylov(Hn, V, 2, apply=dict(col_group=6, tiles=1, threads=1024, blocks_per_sm=1, chunked=0))
     W = torch.randn((Hf.nrows, 256), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
-    device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=4, threads=1024, blocks_per_sm=1, chunked=1))
+    device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1, chunked=0))
     b = torch.randn(Hn.nrows, dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
     device.minres(Hn, b, 1e-300, 1, alpha=-1.0, sigma=40 + 0.6j)
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": "apply", "nnz_Hn": Hn.nnz, "nnz_Hf": Hf.nnz}))
+
+
+def kernel_case_hf_shapes(args):
+    """The H_f apply on 256 columns at six launch shapes (1, 2 or 4 column tiles of 32 per
+    block x interleaved or chunked rows), two launches each: the DRAM cost of wider blocks."""
+    import torch
+    from edrixs_b200 import device
+    m, t = workload_terms(args.nbath, args.nelec)
+    bi = device.fock_unrank(m.nv, args.nelec)
+    Hf = device.build_csr(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=m.nv)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    W = torch.randn((Hf.nrows, 256), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    for tiles in (1, 2, 4):
+        for chunked in (0, 1):
+            device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=tiles, threads=1024, blocks_per_sm=1,
+                                               chunked=chunked))
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": "hf-shapes", "nnz_Hf": Hf.nnz}))
 
 
 def load_peaks():
@@ -112,6 +135,8 @@ def setup_gpu(args, ngs=3):
     e_n, _ = solvers.lowest_eigs(Hn, 1, 1, tol=1e-6)
     edge = float(e_n[0] - gs_e[0])
     P = rixs.RixsProblem(Hn=Hn, Hf=Hf, Din=Din, Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v.contiguous())
+    if not args.no_tiles and not args.c64:
+        P.tiles["hf"] = device.tiles_for(Hf, bi)
     omegas = edge - 2.0 + np.linspace(0.0, 10.0, args.n_omega)
     eloss = np.linspace(-0.5, 12.0, args.n_eloss)
     torch.cuda.synchronize()
@@ -347,9 +372,17 @@ def run_ours(args):
                     launches=launches, total_ms=round(ms, 3))
 
     r_hf = roof(st["hf_nnz"], st["hf_rows"], st["k_hf"], st["hf_apply_ms"], st["hf_iterations"], args.c64)
+    # DRAM bytes per launch from one ncu capture of the same kernel and launch shape on 256 of
+    # the 768 columns (the kernel case above), scaled by the number of 64-column sweeps
+    cfg = tuned.get("hf_k768") or {}
+    if (not st.get("hf_tiled") and not args.c64 and st["k_hf"] == 768 and cfg.get("col_group") == 32
+            and cfg.get("tiles") == 2 and cfg.get("chunked") == 0 and cfg.get("threads") == 1024):
+        r_hf["traffic"] = 3 * 5.725e9
+        r_hf["traffic_source"] = "ncu dram__bytes_read+write on 256 columns (same shape) x 3"
     r_hn = roof(st["hn_nnz"], st["hn_rows"], st["k_hn"], st["hn_apply_ms"], st["hn_iterations"], args.c64)
     dom, sec = (r_hf, r_hn) if r_hf["total_ms"] >= r_hn["total_ms"] else (r_hn, r_hf)
-    dom_name = "k_lanczos_apply on H_f (768 columns)" if dom is r_hf else "k_lanczos_apply on H_n (6 columns)"
+    hf_kernel = "k_lanczos_apply_tiles" if st.get("hf_tiled") else "k_lanczos_apply"
+    dom_name = f"{hf_kernel} on H_f (768 columns)" if dom is r_hf else "k_lanczos_apply on H_n (6 columns)"
 
     extra = {}
     if rank == 0 and not args.no_plain:
@@ -445,7 +478,9 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.kernel_case:
+    if a.kernel_case == "hf-shapes":
+        kernel_case_hf_shapes(a)
+    elif a.kernel_case:
         kernel_case(a)
     elif a.impl == "reference":
         run_reference(a)

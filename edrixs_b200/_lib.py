@@ -42,6 +42,12 @@ class Csr(ctypes.Structure):
                 ("val_type", ctypes.c_int)]
 
 
+class Tiles(ctypes.Structure):
+    _fields_ = [("nrows", i64), ("ntile_r", i32), ("ntile_c", i32), ("tile_r", vp), ("tile_c", vp),
+                ("npiece", i64), ("nent", i64), ("nhdr", i64), ("piece_ptr", vp), ("piece_ctile", vp),
+                ("piece_rows", vp), ("piece_ent", vp), ("piece_hdr", vp), ("hdr", vp), ("lcol", vp), ("val", vp)]
+
+
 class KrylovOpts(ctypes.Structure):
     _fields_ = [("nproj", ctypes.c_int), ("proj", ctypes.POINTER(Csr)), ("proj_out", ctypes.POINTER(vp)),
                 ("nshift", ctypes.c_int), ("shift_col", vp), ("shift_z", vp), ("shift_tol", dbl),
@@ -49,7 +55,8 @@ class KrylovOpts(ctypes.Structure):
                 ("apply_ms", ctypes.POINTER(ctypes.c_double)), ("apply_launches", ctypes.POINTER(ctypes.c_int)),
                 ("apply_col_group", ctypes.c_int), ("apply_threads", ctypes.c_int),
                 ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int),
-                ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int)]
+                ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int),
+                ("apply_layout", ctypes.POINTER(Tiles))]
 
 
 _SIGS = {
@@ -71,6 +78,10 @@ _SIGS = {
                                       ctypes.c_size_t, vp]),
     "edx_spmm": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.c_int, ctypes.c_int, vp, i64, vp, i64, dbl, dbl,
                                 dbl, dbl, dbl, dbl, ctypes.c_int, vp]),
+    "edx_tiles_workspace": (ctypes.c_int, [ctypes.POINTER(Csr), i32, i32, ctypes.POINTER(ctypes.c_size_t)]),
+    "edx_tiles_count": (ctypes.c_int, [ctypes.POINTER(Csr), i32, vp, i32, vp, ctypes.POINTER(i64),
+                                       ctypes.POINTER(i64), ctypes.POINTER(i64), vp, ctypes.c_size_t, vp]),
+    "edx_tiles_fill": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(Tiles), vp, ctypes.c_size_t, vp]),
     "edx_krylov_workspace": (ctypes.c_int, [i64, ctypes.c_int, ctypes.POINTER(KrylovOpts), ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_size_t)]),
     "edx_krylov": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.c_int, vp, ctypes.c_int, vp, vp, vp, vp,

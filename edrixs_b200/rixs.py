@@ -48,12 +48,28 @@ class RixsProblem:
     gs_e: np.ndarray
     gs_v: torch.Tensor                       # (n_i, ngs) complex128
     meta: dict = field(default_factory=dict)
+    tiles: dict = field(default_factory=dict)  # "hf" / "hn" -> device.TiledLayout of that matrix
 
     def nbytes(self):
         b = self.Hn.nbytes() + self.Hf.nbytes() + sum(D.nbytes() for D in self.Din + self.Dout)
         if self.Hn.val64 is not None:
             b += self.Hn.nnz * 8
+        b += sum(L.nbytes() for L in self.tiles.values())
         return b + self.gs_v.numel() * 16
+
+
+def _apply_args(cfg, layout, k, c64):
+    """Launch arguments of one Krylov call: the autotuner's choice, else the tiled product for
+    a wide block (k >= 32) when a layout exists, else libedx's defaults."""
+    if cfg is not None:
+        if cfg.get("tiled"):
+            if layout is None:
+                raise ValueError("the tuned launch shape needs the tiled layout")
+            return dict(layout=layout)
+        return cfg
+    if layout is not None and not c64 and k >= 32:
+        return dict(layout=layout)
+    return None
 
 
 @dataclass
@@ -76,10 +92,10 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     K_hf = npout * k_hn * n_om if final_block is None else int(final_block)
     if autotune:
         from . import tune
-        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64)
-        P.meta[("apply", "hf", K_hf, c64)] = tune.tune_apply(P.Hf, K_hf, c64=c64)
-    cfg_hn = P.meta.get(("apply", "hn", k_hn, c64))
-    cfg_hf = P.meta.get(("apply", "hf", K_hf, c64))
+        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64, layout=P.tiles.get("hn"))
+        P.meta[("apply", "hf", K_hf, c64)] = tune.tune_apply(P.Hf, K_hf, c64=c64, layout=P.tiles.get("hf"))
+    cfg_hn = _apply_args(P.meta.get(("apply", "hn", k_hn, c64)), P.tiles.get("hn"), k_hn, c64)
+    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64)), P.tiles.get("hf"), K_hf, c64)
     gam_c = np.broadcast_to(np.asarray(gamma_c, dtype=np.float64), (n_om,))
     dev = P.gs_v.device
     # 1. seeds (n_n, npin*ngs), column c = p_in*ngs + g
@@ -128,7 +144,7 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
         hf_it += rf.apply_launches
         stats["launches"] += 2 + 3 * rf.apply_launches
     stats.update(hf_apply_ms=hf_ms if timing else None, hf_iterations=hf_it, hf_nnz=P.Hf.nnz, hf_rows=P.Hf.nrows,
-                 k_hf=blk)
+                 k_hf=blk, hf_tiled=bool(cfg_hf and cfg_hf.get("layout") is not None))
     del V0
     # 5. continued fractions; column order (p_out, p_in, g, w)
     e0 = np.tile(np.repeat(np.tile(P.gs_e, npin), n_om), npout)

@@ -38,8 +38,10 @@ def candidates(k):
     return out
 
 
-def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False):
-    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64))
+def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None):
+    """Fastest launch shape for k columns on A.  With a tiled layout of A (complex128 only)
+    the tiled product is timed too and reported as {"tiled": 1}."""
+    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64), layout is not None)
     if key in _cache:
         return _cache[key]
     g = torch.Generator(device=A.val.device)
@@ -47,8 +49,12 @@ def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False):
     V0 = torch.randn((A.nrows, k), dtype=torch.float64, device=A.val.device, generator=g).to(torch.complex128)
     best, best_t = None, float("inf")
     results = []
-    for cfg in candidates(k):
-        r = device.krylov(A, V0, steps, c64=c64, timing=True, apply=cfg)
+    cands = candidates(k)
+    if layout is not None and not c64:
+        cands = [dict(tiled=1)] + cands
+    for cfg in cands:
+        args = dict(layout=layout) if cfg.get("tiled") else cfg
+        r = device.krylov(A, V0, steps, c64=c64, timing=True, apply=args)
         t = r.apply_ms / max(r.apply_launches, 1)
         results.append((t, cfg))
         if t < best_t:

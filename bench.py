@@ -44,7 +44,8 @@ def parse():
     ap.add_argument("--c64", action="store_true", help="complex64 matrices in the Krylov products")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--no-tiles", action="store_true", help="no tiled layout of H_f (CSR product only)")
+    ap.add_argument("--no-packed", action="store_true", help="no packed forms of H_n, H_f (CSR products only)")
+    ap.add_argument("--tiles", action="store_true", help="also offer the tiled layout of H_f to the autotuner")
     ap.add_argument("--kernel-case", choices=["apply", "hf-shapes"], default=None,
                     help="run only a small profiling case of the dominant kernels (for ncu)")
     return ap.parse_args()
@@ -135,8 +136,13 @@ def setup_gpu(args, ngs=3):
     e_n, _ = solvers.lowest_eigs(Hn, 1, 1, tol=1e-6)
     edge = float(e_n[0] - gs_e[0])
     P = rixs.RixsProblem(Hn=Hn, Hf=Hf, Din=Din, Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v.contiguous())
-    if not args.no_tiles and not args.c64:
+    if args.tiles and not args.c64:
         P.tiles["hf"] = device.tiles_for(Hf, bi)
+    if not args.no_packed and not args.c64:
+        for name, M in (("hf", Hf), ("hn", Hn)):
+            pm = device.pack(M)
+            if pm is not None:
+                P.packed[name] = pm
     omegas = edge - 2.0 + np.linspace(0.0, 10.0, args.n_omega)
     eloss = np.linspace(-0.5, 12.0, args.n_eloss)
     torch.cuda.synchronize()
@@ -236,6 +242,17 @@ def cpu_sample(args, t, gs, omega, iters_minres, minres_its=60, krylov_steps=60)
 # arms
 # ------------------------------------------------------------------------------------
 
+def _cf_np(alpha, beta, norm, neff, z):
+    """norm / (z - a0 - b1^2 / (z - a1 - ...)) on the host (the continued fraction of
+    get_spectra_from_poles before its -Im / pi)."""
+    a = alpha[:neff].cpu().numpy()
+    b = beta[:neff].cpu().numpy()
+    g = np.zeros_like(z)
+    for i in range(neff - 1, 0, -1):
+        g = b[i - 1] ** 2 / (z - a[i] - g)
+    return norm / (z - a[0] - g)
+
+
 def accuracy_report(P, res, plain, omegas, eloss, w_idx, nkryl, npin=2, npout=2, ngs=3):
     """Batched vs the plain FP64 one-RHS path at one incident energy, next to the conditioning
     floor of the reference's final-state Lanczos (150 steps, no reorthogonalisation): the
@@ -288,6 +305,34 @@ def accuracy_report(P, res, plain, omegas, eloss, w_idx, nkryl, npin=2, npout=2,
                 floor = max(floor, float(np.abs(sq - sp).max() / scale))
         out["spectra_rel_err"][f"gamma_f_{gamma}"] = err
         out["conditioning_floor"][f"gamma_f_{gamma}"] = floor
+    # both against the exact resolvent -Im <phi|(z - H_f)^-1|phi>, converged MINRES per point:
+    # the 150-step continued fraction's own error, which bounds what "equal to the reference"
+    # can mean pointwise
+    npts = 12
+    pts = np.linspace(0.0, 8.0, npts)
+    for gamma in (1.0, 0.1):
+        eb = ep = 0.0
+        for pi in range(npin):
+            for po in range(npout):
+                se = np.zeros(npts)
+                sb = np.zeros(npts)
+                sp = np.zeros(npts)
+                for g in range(ngs):
+                    b = device.spmm(P.Din[pi], P.gs_v[:, g].contiguous())
+                    z = complex(omegas[w_idx] + P.gs_e[g], 0.6)
+                    x, _, _ = device.minres(P.Hn, b, 1e-10, 1000, alpha=-1.0, sigma=z)
+                    phi = device.spmm(P.Dout[po], x)
+                    zz = pts + P.gs_e[g] + 1j * gamma
+                    nphi = float(torch.linalg.vector_norm(phi))
+                    for q, zq in enumerate(zz):
+                        xe, _, _ = device.minres(P.Hf, phi, 1e-13 * nphi, 60000, alpha=-1.0, sigma=complex(zq))
+                        se[q] += w[g] * -float(torch.vdot(phi, xe).imag)
+                    sb += w[g] * -_cf_np(*batched_set(pi, po, g), zz).imag
+                    sp += w[g] * -_cf_np(*plain_set(pi, po, g), zz).imag
+                scale = np.abs(se).max()
+                eb = max(eb, float(np.abs(sb - se).max() / scale))
+                ep = max(ep, float(np.abs(sp - se).max() / scale))
+        out.setdefault("vs_exact_resolvent", {"points": npts})[f"gamma_f_{gamma}"] = dict(batched=eb, plain=ep)
     # the first Lanczos coefficients, before orthogonality is lost, are well conditioned
     d = 0.0
     for key in plain:
@@ -362,27 +407,37 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     st = stats[-1]
 
-    def roof(nnz, rows, k, ms, launches, c64):
+    def roof(nnz, rows, k, ms, launches, c64, packed=None):
         sv = 8 if c64 else 16
-        per_launch = nnz * (sv + 4) + (rows + 1) * 8 + 3 * k * rows * 16
+        if packed is not None:
+            # what the packed product must read once: entry words, row pointers, diagonal, table
+            per_launch = (packed.ent.numel() * 4 + (rows + 1) * 8 + rows * 16 + packed.vals.numel() * 16
+                          + 3 * k * rows * 16)
+        else:
+            per_launch = nnz * (sv + 4) + (rows + 1) * 8 + 3 * k * rows * 16
         avg_ms = ms / max(launches, 1)
         ach = per_launch / (avg_ms / 1e3) / 1e9
         return dict(bound="hbm", achieved=round(ach, 1), peak=peak, unit="GB/s", frac=round(ach / peak, 4),
                     traffic=None, bytes_per_launch=int(per_launch), avg_launch_us=round(avg_ms * 1e3, 2),
                     launches=launches, total_ms=round(ms, 3))
 
-    r_hf = roof(st["hf_nnz"], st["hf_rows"], st["k_hf"], st["hf_apply_ms"], st["hf_iterations"], args.c64)
+    r_hf = roof(st["hf_nnz"], st["hf_rows"], st["k_hf"], st["hf_apply_ms"], st["hf_iterations"], args.c64,
+                P.packed.get("hf") if st.get("hf_packed") else None)
     # DRAM bytes per launch from one ncu capture of the same kernel and launch shape on 256 of
     # the 768 columns (the kernel case above), scaled by the number of 64-column sweeps
     cfg = tuned.get("hf_k768") or {}
-    if (not st.get("hf_tiled") and not args.c64 and st["k_hf"] == 768 and cfg.get("col_group") == 32
+    if (not st.get("hf_tiled") and not st.get("hf_packed") and not args.c64 and st["k_hf"] == 768
+            and cfg.get("col_group") == 32
             and cfg.get("tiles") == 2 and cfg.get("chunked") == 0 and cfg.get("threads") == 1024):
         r_hf["traffic"] = 3 * 5.725e9
         r_hf["traffic_source"] = "ncu dram__bytes_read+write on 256 columns (same shape) x 3"
-    r_hn = roof(st["hn_nnz"], st["hn_rows"], st["k_hn"], st["hn_apply_ms"], st["hn_iterations"], args.c64)
+    r_hn = roof(st["hn_nnz"], st["hn_rows"], st["k_hn"], st["hn_apply_ms"], st["hn_iterations"], args.c64,
+                P.packed.get("hn") if st.get("hn_packed") else None)
     dom, sec = (r_hf, r_hn) if r_hf["total_ms"] >= r_hn["total_ms"] else (r_hn, r_hf)
-    hf_kernel = "k_lanczos_apply_tiles" if st.get("hf_tiled") else "k_lanczos_apply"
-    dom_name = f"{hf_kernel} on H_f (768 columns)" if dom is r_hf else "k_lanczos_apply on H_n (6 columns)"
+    hf_kernel = ("k_lanczos_apply_tiles" if st.get("hf_tiled") else
+                 "k_lanczos_apply_packed" if st.get("hf_packed") else "k_lanczos_apply")
+    hn_kernel = "k_lanczos_apply_packed" if st.get("hn_packed") else "k_lanczos_apply"
+    dom_name = f"{hf_kernel} on H_f (768 columns)" if dom is r_hf else f"{hn_kernel} on H_n (6 columns)"
 
     extra = {}
     if rank == 0 and not args.no_plain:
@@ -432,7 +487,8 @@ def run_ours(args):
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": dict(dom, kernel=dom_name, peak_source=peak_kind),
-            "roofline_secondary": dict(sec, kernel="k_lanczos_apply (other phase)"),
+            "roofline_secondary": dict(sec, kernel=(f"{hn_kernel} on H_n (6 columns)" if sec is r_hn
+                                                    else f"{hf_kernel} on H_f (768 columns)")),
             "gpu_launches": int(sum(s["launches"] for s in stats)),
             "minres_iterations": {"mean": float(np.mean(res.iters)), "max": int(np.max(res.iters))},
             "clocks": clocks,

@@ -48,6 +48,11 @@ class Tiles(ctypes.Structure):
                 ("piece_rows", vp), ("piece_ent", vp), ("piece_hdr", vp), ("hdr", vp), ("lcol", vp), ("val", vp)]
 
 
+class Packed(ctypes.Structure):
+    _fields_ = [("nrows", i64), ("nnz", i64), ("row_ptr", vp), ("ent", vp), ("vbits", ctypes.c_int),
+                ("nval", ctypes.c_int), ("vals", vp), ("diag", vp)]
+
+
 class KrylovOpts(ctypes.Structure):
     _fields_ = [("nproj", ctypes.c_int), ("proj", ctypes.POINTER(Csr)), ("proj_out", ctypes.POINTER(vp)),
                 ("nshift", ctypes.c_int), ("shift_col", vp), ("shift_z", vp), ("shift_tol", dbl),
@@ -56,7 +61,7 @@ class KrylovOpts(ctypes.Structure):
                 ("apply_col_group", ctypes.c_int), ("apply_threads", ctypes.c_int),
                 ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int),
                 ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int),
-                ("apply_layout", ctypes.POINTER(Tiles))]
+                ("apply_layout", ctypes.POINTER(Tiles)), ("apply_packed", ctypes.POINTER(Packed))]
 
 
 _SIGS = {
@@ -82,6 +87,10 @@ _SIGS = {
     "edx_tiles_count": (ctypes.c_int, [ctypes.POINTER(Csr), i32, vp, i32, vp, ctypes.POINTER(i64),
                                        ctypes.POINTER(i64), ctypes.POINTER(i64), vp, ctypes.c_size_t, vp]),
     "edx_tiles_fill": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(Tiles), vp, ctypes.c_size_t, vp]),
+    "edx_pack_workspace": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(ctypes.c_size_t)]),
+    "edx_pack_count": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int), vp, ctypes.c_size_t, vp]),
+    "edx_pack_fill": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(Packed), vp, ctypes.c_size_t, vp]),
     "edx_krylov_workspace": (ctypes.c_int, [i64, ctypes.c_int, ctypes.POINTER(KrylovOpts), ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_size_t)]),
     "edx_krylov": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.c_int, vp, ctypes.c_int, vp, vp, vp, vp,

@@ -69,6 +69,11 @@ struct KrylovState {
     int* n_active;      // [1]
     double* part;       // [GX*k]
     unsigned* ticket;   // [4]
+    // The Lanczos vectors are stored unnormalised: v_i = scur * U_i (U_i = the orthogonalised
+    // residual of the previous step) and v_{i-1} = sprev * U_{i-1}; the products and the
+    // orthogonalisation apply the scales on the fly, so no separate normalisation pass runs.
+    double* scur;       // [k] 1/beta_{i-1} (0 for stopped columns)
+    double* sprev;      // [k] 1/beta_{i-2}
     int maxn, k;
 };
 
@@ -90,11 +95,12 @@ __global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* 
     const int c = lane % KW;
     const int k = S.k;
     const int col0 = blockIdx.y * BC;
-    double bprev[TG], apart[TG];
+    double bprev[TG], scur[TG], apart[TG];
 #pragma unroll
     for (int g = 0; g < TG; ++g) {
         const int gc = col0 + g * KW + c;
-        bprev[g] = (gc < k && it > 0) ? S.beta[gc] : 0.0;
+        bprev[g] = (gc < k && it > 0) ? S.beta[gc] * S.sprev[gc] : 0.0;
+        scur[g] = gc < k ? S.scur[gc] : 0.0;
         apart[g] = 0.0;
     }
     int64_t r0, r1, rstep;
@@ -124,13 +130,13 @@ __global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* 
                 const int gc = col0 + g * KW + c;
                 if (gc < k) {
                     const int64_t o = r * k + gc;
-                    double2 vp = Vp[o];
+                    const double2 vp = Vp[o];
                     double2 w = make_double2(-bprev[g] * vp.x, -bprev[g] * vp.y);
-                    w.x = w.x + acc[g].x;
-                    w.y = w.y + acc[g].y;
+                    w.x = w.x + scur[g] * acc[g].x;
+                    w.y = w.y + scur[g] * acc[g].y;
                     Vp[o] = w;
-                    double2 vc = Vc[o];
-                    apart[g] += vc.x * w.x + vc.y * w.y;  // Re(conj(v) w)
+                    const double2 vc = Vc[o];
+                    apart[g] += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
                 }
             }
         }
@@ -149,7 +155,96 @@ __global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* 
     __syncthreads();
     if (arrive_last(S.ticket)) {
         for (int j = threadIdx.x; j < k; j += NT) {
-            double a = sum_partials(S.part, gridDim.x, k, j);
+            const double a = S.scur[j] * sum_partials(S.part, gridDim.x, k, j);
+            S.alpha[j] = a;
+            if (S.active[j]) S.alpha_out[(int64_t)j * S.maxn + it] = a;
+        }
+        if (threadIdx.x == 0) *S.ticket = 0u;
+    }
+}
+
+// ---- K9a on the packed form ---------------------------------------------------------------
+// Same row mapping and epilogue as k_lanczos_apply.  The distinct values are copied to shared
+// memory first; the diagonal term d_r v_r is added in the epilogue, where V_cur[r] is read
+// anyway for alpha.
+struct PackedView {
+    const int64_t* row_ptr;
+    const uint32_t* ent;
+    const double2* vals;
+    const double2* diag;
+    int vbits, nval;
+};
+
+template <int KW, int TG, int NT>
+__global__ void __launch_bounds__(NT) k_lanczos_apply_packed(int64_t n, PackedView M, const double2* __restrict__ Vc,
+                                                             double2* __restrict__ Vp, KrylovState S, int it,
+                                                             int chunked) {
+    constexpr int NW = NT / 32;
+    constexpr int BC = TG * KW;
+    extern __shared__ double2 pk_tab[];
+    __shared__ double sh[NW * BC];
+    for (int i = threadIdx.x; i < M.nval; i += NT) pk_tab[i] = M.vals[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c = lane % KW;
+    const int k = S.k;
+    const int col0 = blockIdx.y * BC;
+    double bprev[TG], scur[TG], apart[TG];
+#pragma unroll
+    for (int g = 0; g < TG; ++g) {
+        const int gc = col0 + g * KW + c;
+        bprev[g] = (gc < k && it > 0) ? S.beta[gc] * S.sprev[gc] : 0.0;
+        scur[g] = gc < k ? S.scur[gc] : 0.0;
+        apart[g] = 0.0;
+    }
+    int64_t r0, r1, rstep;
+    if (chunked) {
+        const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+        r0 = (int64_t)blockIdx.x * per + warp;
+        r1 = min(n, (int64_t)(blockIdx.x + 1) * per);
+        rstep = NW;
+    } else {
+        r0 = (int64_t)blockIdx.x * NW + warp;
+        r1 = n;
+        rstep = (int64_t)gridDim.x * NW;
+    }
+    for (int64_t r = r0; r < r1; r += rstep) {
+        const int64_t s = __ldg(M.row_ptr + r), e = __ldg(M.row_ptr + r + 1);
+        double2 acc[TG];
+        row_times_x_packed<KW, TG>(s, e, M.ent, M.vbits, pk_tab, Vc, k, col0, k, acc);
+        if (lane < KW) {
+            const double2 d = __ldg(M.diag + r);
+#pragma unroll
+            for (int g = 0; g < TG; ++g) {
+                const int gc = col0 + g * KW + c;
+                if (gc < k) {
+                    const int64_t o = r * k + gc;
+                    const double2 vc = Vc[o];
+                    const double2 hv = fma_c(d, vc, acc[g]);
+                    const double2 vp = Vp[o];
+                    double2 w = make_double2(-bprev[g] * vp.x, -bprev[g] * vp.y);
+                    w.x = w.x + scur[g] * hv.x;
+                    w.y = w.y + scur[g] * hv.y;
+                    Vp[o] = w;
+                    apart[g] += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
+                }
+            }
+        }
+    }
+    if (lane < KW) {
+#pragma unroll
+        for (int g = 0; g < TG; ++g) sh[warp * BC + g * KW + lane] = apart[g];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < BC; i += NT) {
+        double s = 0.0;
+        for (int w = 0; w < NW; ++w) s += sh[w * BC + i];
+        if (col0 + i < k) S.part[(int64_t)blockIdx.x * k + col0 + i] = s;
+    }
+    __syncthreads();
+    if (arrive_last(S.ticket)) {
+        for (int j = threadIdx.x; j < k; j += NT) {
+            const double a = S.scur[j] * sum_partials(S.part, gridDim.x, k, j);
             S.alpha[j] = a;
             if (S.active[j]) S.alpha_out[(int64_t)j * S.maxn + it] = a;
         }
@@ -304,7 +399,8 @@ __global__ void __launch_bounds__(TL_NT, 1)
     // W = A V_cur - beta_{i-1} V_prev into V_prev; alpha partial Re(conj(v) w) per column
     const int gc = col0 + lane;
     const bool ok = gc < k;
-    const double bprev = (ok && it > 0) ? S.beta[gc] : 0.0;
+    const double bprev = (ok && it > 0) ? S.beta[gc] * S.sprev[gc] : 0.0;
+    const double scur = ok ? S.scur[gc] : 0.0;
     double apart = 0.0;
 #pragma unroll
     for (int t = 0; t < TL_RPW; ++t) {
@@ -313,8 +409,8 @@ __global__ void __launch_bounds__(TL_NT, 1)
             const int64_t o = (int64_t)(r0 + lr) * k + gc;
             const double2 vp = Vp[o];
             double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
-            w.x = w.x + acc[t].x;
-            w.y = w.y + acc[t].y;
+            w.x = w.x + scur * acc[t].x;
+            w.y = w.y + scur * acc[t].y;
             Vp[o] = w;
             const double2 vc = Vc[o];
             apart += vc.x * w.x + vc.y * w.y;
@@ -347,6 +443,7 @@ __global__ void __launch_bounds__(TL_NT, 1)
         double a = 0.0;
         for (int w = 0; w < TL_NW; ++w) a += sh[w * 32 + lane];
         if (ok) {
+            a *= scur;
             S.alpha[gc] = a;
             if (S.active[gc]) S.alpha_out[(int64_t)gc * S.maxn + it] = a;
         }
@@ -354,15 +451,21 @@ __global__ void __launch_bounds__(TL_NT, 1)
     }
 }
 
-// ---- K9b: W -= alpha V_cur, beta = |W| ------------------------------------------------
+// ---- K9b: W -= alpha v_i, beta = |W|, next scales -----------------------------------------
+// v_i = scur * U_i, so W -= (alpha * scur) U_i.  The last block of each column group (one
+// ticket per group) finishes its columns: beta from the per-block partials (the group's
+// threads each add a fixed subset of the blocks, then one thread adds the subsets in order),
+// the reference's stopping rule (|beta| < 1e-10), the scales of the next step and its share
+// of the active-column count.
 template <int KW>
 __global__ void __launch_bounds__(KT) k_lanczos_orth(int64_t n, const double2* __restrict__ Vc,
-                                                     double2* __restrict__ Vp, KrylovState S, int it) {
+                                                     double2* __restrict__ Vp, KrylovState S,
+                                                     unsigned* __restrict__ gticket, int it) {
     const int k = S.k;
     const int c = threadIdx.x % KW, g = threadIdx.x / KW, groups = KT / KW;
     const int gc = blockIdx.y * KW + c;
     const bool colok = gc < k;
-    const double a = colok ? S.alpha[gc] : 0.0;
+    const double a = colok ? S.alpha[gc] * S.scur[gc] : 0.0;
     double part = 0.0;
     if (colok) {
         for (int64_t r = (int64_t)blockIdx.x * groups + g; r < n; r += (int64_t)gridDim.x * groups) {
@@ -375,48 +478,56 @@ __global__ void __launch_bounds__(KT) k_lanczos_orth(int64_t n, const double2* _
         }
     }
     block_col_partial<KW>(part, true, g, groups, c, k, S.part);
-    if (arrive_last(S.ticket + 1)) {
-        int cnt = 0;
-        for (int j = threadIdx.x; j < k; j += KT) {
-            double b = sqrt(sum_partials(S.part, gridDim.x, k, j));
-            if (S.active[j]) {
-                S.beta_out[(int64_t)j * S.maxn + it] = b;
-                S.neff[j] = it + 1;
-                if (fabs(b) < 1e-10) S.active[j] = 0;
-            }
-            S.beta[j] = b;
-            cnt += S.active[j];
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(gticket + blockIdx.y, 1u) == gridDim.x - 1u);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double red[KT];
+    double sub = 0.0;
+    if (colok)
+        for (int b = g; b < (int)gridDim.x; b += groups) sub += __ldcg(S.part + (int64_t)b * k + gc);
+    red[threadIdx.x] = sub;
+    __syncthreads();
+    int act = 0;
+    if (threadIdx.x < KW && colok) {
+        double tot = 0.0;
+        for (int q = 0; q < groups; ++q) tot += red[q * KW + c];
+        const double b = sqrt(tot);
+        const int j = gc;
+        if (S.active[j]) {
+            S.beta_out[(int64_t)j * S.maxn + it] = b;
+            S.neff[j] = it + 1;
+            if (fabs(b) < 1e-10) S.active[j] = 0;
         }
-        // count active columns
-        __shared__ int scnt[KT];
-        scnt[threadIdx.x] = cnt;
-        __syncthreads();
+        S.beta[j] = b;
+        S.sprev[j] = S.scur[j];
+        S.scur[j] = S.active[j] ? 1.0 / b : 0.0;
+        act = S.active[j];
+    }
+    if (threadIdx.x < 32) {
+        act = __reduce_add_sync(0xffffffffu, act);
         if (threadIdx.x == 0) {
-            int t = 0;
-            for (int q = 0; q < KT; ++q) t += scnt[q];
-            *S.n_active = t;
-            S.ticket[1] = 0u;
+            if (act) atomicAdd(S.n_active, act);
+            gticket[blockIdx.y] = 0u;
         }
     }
 }
 
-// ---- K9c: V_next = W / beta (inactive columns -> 0) ------------------------------------
-__global__ void k_lanczos_scale(int64_t n, int k, double2* __restrict__ Vp, const double* __restrict__ beta,
-                                const int* __restrict__ active) {
-    const int64_t total = n * k;
+// projections of U_i scaled to v_i = scur * U_i: out[(j*maxn + i)*m + r] *= scur[j]
+__global__ void k_proj_scale(int64_t m, int k, int64_t maxn, int i, double2* __restrict__ out,
+                             const double* __restrict__ scur) {
+    const int64_t total = m * k;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % k);
-        double2 w = Vp[e];
-        if (active[c]) {
-            const double b = beta[c];
-            w.x = w.x / b;
-            w.y = w.y / b;
-        } else {
-            w.x = 0.0;
-            w.y = 0.0;
-        }
-        Vp[e] = w;
+        const int j = (int)(e / m);
+        const int64_t r = e - (int64_t)j * m;
+        double2* p = out + ((int64_t)j * maxn + i) * m + r;
+        const double f = scur[j];
+        double2 v = *p;
+        *p = make_double2(v.x * f, v.y * f);
     }
 }
 
@@ -440,6 +551,8 @@ __global__ void __launch_bounds__(KT) k_colnorm(int64_t n, const double2* __rest
             S.beta[j] = sqrt(s);
             S.active[j] = 1;
             S.neff[j] = 0;
+            S.scur[j] = 1.0;  // v_0 is stored normalised
+            S.sprev[j] = 0.0;
         }
         if (threadIdx.x == 0) S.ticket[2] = 0u;
     }
@@ -605,6 +718,57 @@ static int apply_v(const edx_csr* A, const double2* Vc, double2* Vp, const Krylo
     return fail(EDX_ERR_INVALID, "krylov: bad column group %d", cfg.kw);
 }
 
+template <int KW, int TG, int NT>
+static int launch_packed_nt(int64_t n, const PackedView& M, const double2* Vc, double2* Vp, const KrylovState& S,
+                            int it, const ApplyCfg& cfg, cudaStream_t st) {
+    auto kern = k_lanczos_apply_packed<KW, TG, NT>;
+    static bool attr_set[EDX_MAX_DEVICES] = {};
+    int dev = 0;
+    EDX_CUDA(cudaGetDevice(&dev));
+    EDX_REQUIRE(dev >= 0 && dev < EDX_MAX_DEVICES, "edx_krylov: device ordinal %d out of range", dev);
+    if (!attr_set[dev]) {
+        EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(EDX_PACK_VALUES_MAX * sizeof(double2))));
+        attr_set[dev] = true;
+    }
+    const int ntiles = (S.k + KW - 1) / KW;
+    dim3 grid(cfg.gx, (ntiles + TG - 1) / TG);
+    kern<<<grid, NT, (size_t)M.nval * sizeof(double2), st>>>(n, M, Vc, Vp, S, it, cfg.chunked);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}
+
+template <int KW, int TG>
+static int launch_packed(int64_t n, const PackedView& M, const double2* Vc, double2* Vp, const KrylovState& S,
+                         int it, const ApplyCfg& cfg, cudaStream_t st) {
+    if (cfg.threads == 1024) return launch_packed_nt<KW, TG, 1024>(n, M, Vc, Vp, S, it, cfg, st);
+    return launch_packed_nt<KW, TG, 256>(n, M, Vc, Vp, S, it, cfg, st);
+}
+
+static int apply_packed(const edx_packed* P, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+                        const ApplyCfg& cfg, cudaStream_t st) {
+    const PackedView M{P->row_ptr, P->ent, reinterpret_cast<const double2*>(P->vals),
+                       reinterpret_cast<const double2*>(P->diag), P->vbits, P->nval};
+    const int64_t n = P->nrows;
+    switch (cfg.kw) {
+    case 1: return launch_packed<1, 1>(n, M, Vc, Vp, S, it, cfg, st);
+    case 2: return launch_packed<2, 1>(n, M, Vc, Vp, S, it, cfg, st);
+    case 4: return launch_packed<4, 1>(n, M, Vc, Vp, S, it, cfg, st);
+    case 6: return launch_packed<6, 1>(n, M, Vc, Vp, S, it, cfg, st);
+    case 8: return launch_packed<8, 1>(n, M, Vc, Vp, S, it, cfg, st);
+    case 12: return launch_packed<12, 1>(n, M, Vc, Vp, S, it, cfg, st);
+    case 16:
+        if (cfg.tg == 4) return launch_packed<16, 4>(n, M, Vc, Vp, S, it, cfg, st);
+        if (cfg.tg == 2) return launch_packed<16, 2>(n, M, Vc, Vp, S, it, cfg, st);
+        return launch_packed<16, 1>(n, M, Vc, Vp, S, it, cfg, st);
+    case 32:
+        if (cfg.tg == 4) return launch_packed<32, 4>(n, M, Vc, Vp, S, it, cfg, st);
+        if (cfg.tg == 2) return launch_packed<32, 2>(n, M, Vc, Vp, S, it, cfg, st);
+        return launch_packed<32, 1>(n, M, Vc, Vp, S, it, cfg, st);
+    }
+    return fail(EDX_ERR_INVALID, "krylov: bad column group %d", cfg.kw);
+}
+
 static int apply_tiles(const edx_tiles* L, const double2* Vc, double2* Vp, const KrylovState& S, unsigned* gt,
                        int it, cudaStream_t st) {
     static bool smem_set[EDX_MAX_DEVICES] = {};
@@ -637,7 +801,7 @@ static int apply_tiles(const edx_tiles* L, const double2* Vc, double2* Vp, const
 
 struct KrylovWs {
     double2 *Vc, *Vp;
-    double *alpha, *beta, *part;
+    double *alpha, *beta, *part, *scur, *sprev;
     int *active, *n_active, *n_open;
     unsigned* ticket;
     unsigned* gticket;  // one per 32 columns (tiled product)
@@ -659,6 +823,8 @@ static void krylov_layout(WS& w, int64_t n, int k, int nshift, int maxn, int gx,
     auto Vp = w.template take<double2>((size_t)(n * k));
     auto al = w.template take<double>((size_t)k);
     auto be = w.template take<double>((size_t)k);
+    auto sc = w.template take<double>((size_t)k);
+    auto sp = w.template take<double>((size_t)k);
     auto pa = w.template take<double>((size_t)gx * k);
     auto ac = w.template take<int>((size_t)k);
     auto na = w.template take<int>(2);
@@ -671,6 +837,8 @@ static void krylov_layout(WS& w, int64_t n, int k, int nshift, int maxn, int gx,
         out->Vp = Vp;
         out->alpha = al;
         out->beta = be;
+        out->scur = sc;
+        out->sprev = sp;
         out->part = pa;
         out->active = ac;
         out->n_active = na;
@@ -751,6 +919,13 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
                     "edx_krylov: apply_layout does not describe this matrix");
         EDX_REQUIRE((k + 31) / 32 <= 65535, "edx_krylov: too many columns for the tiled product");
     }
+    const edx_packed* packed = opts ? opts->apply_packed : nullptr;
+    if (packed) {
+        EDX_REQUIRE(packed->nrows == n && packed->row_ptr && packed->diag &&
+                        (packed->nnz == 0 || (packed->ent && packed->vals)) && packed->nval >= 0 &&
+                        packed->nval <= EDX_PACK_VALUES_MAX && packed->vbits >= 1 && packed->vbits <= 31,
+                    "edx_krylov: apply_packed does not describe this matrix");
+    }
     const int kw = pow2_kw(k);  // layout of the element-wise recurrence kernels
     const int gy = (k + kw - 1) / kw;
     int gx = num_sms() * 8;
@@ -770,6 +945,8 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     S.n_active = ws.n_active;
     S.part = ws.part;
     S.ticket = ws.ticket;
+    S.scur = ws.scur;
+    S.sprev = ws.sprev;
     S.maxn = maxn;
     S.k = k;
 
@@ -801,6 +978,13 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
             int r2 = spmm_dispatch(P, k, EDX_C128, V, k, out, 1, (int64_t)maxn * P->nrows,
                                    make_double2(1, 0), make_double2(0, 0), make_double2(0, 0), 0, st);
             if (r2) return r2;
+            if (i > 0) {  // the stored vectors are unnormalised: scale to v_i
+                const int64_t tot = P->nrows * (int64_t)k;
+                const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)num_sms() * 8);
+                k_proj_scale<<<blocks, 256, 0, st>>>(P->nrows, k, maxn, i,
+                                                     reinterpret_cast<double2*>(opts->proj_out[p]), ws.scur);
+                EDX_CHECK_LAUNCH();
+            }
         }
         return EDX_OK;
     };
@@ -817,7 +1001,8 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     };
     int launches = 0;
     for (int it = 0; it < maxn; ++it) {
-        if (nshift > 0) EDX_CUDA(cudaMemsetAsync(ws.n_open, 0, sizeof(int), st));
+        // active-column count (summed by the orthogonalisation) and open-shift count
+        EDX_CUDA(cudaMemsetAsync(ws.n_active, 0, (nshift > 0 ? 2 : 1) * sizeof(int), st));
         if (timed) {
             cudaEvent_t e0, e1;
             EDX_CUDA(cudaEventCreate(&e0));
@@ -828,6 +1013,8 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
         }
         if (layout)
             rc = apply_tiles(layout, Vc, Vp, S, ws.gticket, it, st);
+        else if (packed)
+            rc = apply_packed(packed, Vc, Vp, S, it, cfg, st);
         else
             rc = (A->val_type == EDX_C128) ? apply_v<double2>(A, Vc, Vp, S, it, cfg, st)
                                            : apply_v<float2>(A, Vc, Vp, S, it, cfg, st);
@@ -839,7 +1026,7 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
         ++launches;
         {
             dim3 grid(reduce_grid(n), gy);
-            EDX_KW_SWITCH(kw, k_lanczos_orth, grid, n, Vc, Vp, S, it);
+            EDX_KW_SWITCH(kw, k_lanczos_orth, grid, n, Vc, Vp, S, ws.gticket, it);
             EDX_CHECK_LAUNCH();
         }
         if (nshift > 0) {
@@ -848,8 +1035,6 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
                 reinterpret_cast<double2*>(opts->shift_y), S, it, opts->shift_tol, opts->shift_maxit, ws.n_open);
             EDX_CHECK_LAUNCH();
         }
-        k_lanczos_scale<<<eb, 256, 0, st>>>(n, k, Vp, ws.beta, ws.active);
-        EDX_CHECK_LAUNCH();
         std::swap(Vc, Vp);
         if (it + 1 < maxn && (rc = project(Vc, it + 1))) return rc;
         if ((it + 1) % poll == 0 || it + 1 == maxn) {

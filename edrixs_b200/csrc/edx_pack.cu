@@ -1,0 +1,294 @@
+// edx_pack.cu -- packed form of a square complex128 matrix: dense diagonal, one 32-bit word
+// per off-diagonal entry (column << vbits | index into the table of distinct values).
+//
+// Count pass: split diagonal / off-diagonal (CSR order kept), sort the off-diagonal value
+// bit patterns lexicographically (two stable radix sorts: imaginary bits, then real bits),
+// flag the first of every run of equal patterns and scan the flags: the distinct values in
+// ascending bit order form the table.  Fill pass: every entry finds its value in the table
+// by binary search over the same bit patterns, so values are carried bit for bit.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+
+#include "edx_common.cuh"
+
+namespace edx {
+
+int check_csr(const edx_csr* A);
+
+namespace {
+
+__device__ __forceinline__ uint64_t bits_of(double v) { return (uint64_t)__double_as_longlong(v); }
+
+// off-diagonal entries per row (the CSR holds at most one diagonal entry per row)
+__global__ void k_pk_count(int64_t n, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                           int64_t* __restrict__ cnt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t ws = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = w0; r < n; r += ws) {
+        const int64_t s = row_ptr[r], e = row_ptr[r + 1];
+        int d = 0;
+        for (int64_t j = s + lane; j < e; j += 32) d += (col[j] == r);
+        d = __reduce_add_sync(0xffffffffu, d);
+        if (lane == 0) cnt[r] = (e - s) - d;
+    }
+}
+
+// diagonal into diag, off-diagonal value bits (re, im) into the key arrays at off_ptr[r] + i
+__global__ void k_pk_split(int64_t n, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                           const double2* __restrict__ val, const int64_t* __restrict__ off_ptr,
+                           double2* __restrict__ diag, uint64_t* __restrict__ re, uint64_t* __restrict__ im) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t ws = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = w0; r < n; r += ws) {
+        const int64_t s = row_ptr[r], e = row_ptr[r + 1];
+        int64_t o = off_ptr[r];
+        double2 dg = make_double2(0.0, 0.0);
+        for (int64_t base = s; base < e; base += 32) {
+            const int64_t j = base + lane;
+            const bool in = j < e;
+            const bool isd = in && col[j] == r;
+            const bool off = in && !isd;
+            const double2 v = in ? val[j] : make_double2(0.0, 0.0);
+            const unsigned md = __ballot_sync(0xffffffffu, isd);
+            if (md) dg = shfl2(v, __ffs(md) - 1);
+            const unsigned m = __ballot_sync(0xffffffffu, off);
+            if (off) {
+                const int64_t q = o + __popc(m & ((1u << lane) - 1u));
+                re[q] = bits_of(v.x);
+                im[q] = bits_of(v.y);
+            }
+            o += __popc(m);
+        }
+        if (lane == 0) diag[r] = dg;
+    }
+}
+
+__global__ void k_pk_flags(int64_t m, const uint64_t* __restrict__ re, const uint64_t* __restrict__ im,
+                           int32_t* __restrict__ flag) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        flag[i] = (i == 0 || re[i] != re[i - 1] || im[i] != im[i - 1]) ? 1 : 0;
+}
+
+__global__ void k_pk_table(int64_t m, const uint64_t* __restrict__ re, const uint64_t* __restrict__ im,
+                           const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
+                           uint64_t* __restrict__ tre, uint64_t* __restrict__ tim, int32_t* __restrict__ count) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        if (flag[i] && pos[i] < EDX_PACK_VALUES_MAX) {
+            tre[pos[i]] = re[i];
+            tim[pos[i]] = im[i];
+        }
+        if (i == m - 1) *count = pos[i] + flag[i];
+    }
+}
+
+// warp per row: pack every off-diagonal entry; the value index by binary search in the table
+__global__ void k_pk_fill(int64_t n, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
+                          const double2* __restrict__ val, const int64_t* __restrict__ off_ptr,
+                          const uint64_t* __restrict__ tre, const uint64_t* __restrict__ tim, int nval, int vbits,
+                          uint32_t* __restrict__ ent) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t ws = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = w0; r < n; r += ws) {
+        const int64_t s = row_ptr[r], e = row_ptr[r + 1];
+        int64_t o = off_ptr[r];
+        for (int64_t base = s; base < e; base += 32) {
+            const int64_t j = base + lane;
+            const bool off = j < e && col[j] != r;
+            const unsigned m = __ballot_sync(0xffffffffu, off);
+            if (off) {
+                const double2 v = val[j];
+                const uint64_t a = bits_of(v.x), b = bits_of(v.y);
+                int lo = 0, hi = nval - 1;
+                while (lo < hi) {  // first table slot >= (a, b)
+                    const int mid = (lo + hi) >> 1;
+                    const uint64_t ta = tre[mid], tb = tim[mid];
+                    if (ta < a || (ta == a && tb < b)) lo = mid + 1;
+                    else hi = mid;
+                }
+                const int64_t q = o + __popc(m & ((1u << lane) - 1u));
+                ent[q] = ((uint32_t)col[j] << vbits) | (uint32_t)lo;
+            }
+            o += __popc(m);
+        }
+    }
+}
+
+__global__ void k_pk_vals(int nval, const uint64_t* __restrict__ tre, const uint64_t* __restrict__ tim,
+                          double2* __restrict__ vals) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nval) vals[i] = make_double2(__longlong_as_double((long long)tre[i]), __longlong_as_double((long long)tim[i]));
+}
+
+struct PackWs {
+    int64_t *cnt, *off_ptr;
+    double2* diag;
+    uint64_t *re0, *im0, *re1, *im1, *tre, *tim;
+    int32_t *flag, *pos, *count;
+    void* temp;
+    size_t temp_bytes;
+};
+
+int pack_temp_bytes(int64_t n, int64_t nnz, size_t* out) {
+    size_t a = 0, b = 0, c = 0;
+    EDX_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, a, (const int64_t*)nullptr, (int64_t*)nullptr, (int)(n + 1)));
+    EDX_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                             (const uint64_t*)nullptr, (uint64_t*)nullptr, (int)nnz));
+    EDX_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, c, (const int32_t*)nullptr, (int32_t*)nullptr, (int)nnz));
+    *out = std::max(a, std::max(b, c));
+    return EDX_OK;
+}
+
+template <class WS>
+void pack_layout(WS& w, int64_t n, int64_t nnz, size_t temp, PackWs* o) {
+    auto cnt = w.template take<int64_t>((size_t)n + 1);
+    auto off = w.template take<int64_t>((size_t)n + 1);
+    auto dg = w.template take<double2>((size_t)n);
+    auto re0 = w.template take<uint64_t>((size_t)nnz);
+    auto im0 = w.template take<uint64_t>((size_t)nnz);
+    auto re1 = w.template take<uint64_t>((size_t)nnz);
+    auto im1 = w.template take<uint64_t>((size_t)nnz);
+    auto fl = w.template take<int32_t>((size_t)nnz);
+    auto ps = w.template take<int32_t>((size_t)nnz);
+    auto tre = w.template take<uint64_t>(EDX_PACK_VALUES_MAX);
+    auto tim = w.template take<uint64_t>(EDX_PACK_VALUES_MAX);
+    auto ct = w.template take<int32_t>(4);
+    auto tmp = w.template take<char>(temp);
+    if (o) *o = PackWs{cnt, off, dg, re0, im0, re1, im1, tre, tim, fl, ps, ct, tmp, temp};
+}
+
+struct SizeOnlyP {
+    WorkspaceSize s;
+    template <class T>
+    T* take(size_t c) {
+        s.take<T>(c);
+        return nullptr;
+    }
+};
+
+int check_square(const edx_csr* A) {
+    int rc = check_csr(A);
+    if (rc) return rc;
+    EDX_REQUIRE(A->nrows == A->ncols && A->nrows >= 1, "edx_pack: matrix must be square and non-empty");
+    EDX_REQUIRE(A->val_type == EDX_C128, "edx_pack: complex128 matrices only");
+    EDX_REQUIRE(A->nnz >= 1 && A->nnz < ((int64_t)1 << 31), "edx_pack: nnz must be 1 .. 2^31-1");
+    return EDX_OK;
+}
+
+int value_bits(int64_t ncols) {
+    int cb = 1;
+    while (cb < 32 && ((int64_t)1 << cb) < ncols) ++cb;
+    return 32 - cb;
+}
+
+}  // namespace
+}  // namespace edx
+
+using namespace edx;
+
+extern "C" int edx_pack_workspace(const edx_csr* A, size_t* bytes) {
+    int rc = check_square(A);
+    if (rc) return rc;
+    EDX_REQUIRE(bytes, "edx_pack_workspace: bytes missing");
+    size_t temp = 0;
+    if ((rc = pack_temp_bytes(A->nrows, A->nnz, &temp))) return rc;
+    SizeOnlyP s;
+    pack_layout(s, A->nrows, A->nnz, temp, nullptr);
+    *bytes = s.s.bytes();
+    return EDX_OK;
+}
+
+extern "C" int edx_pack_count(const edx_csr* A, int64_t* nnz_off, int* nval, int* vbits, void* d_work,
+                              size_t work_bytes, void* stream) {
+    int rc = check_square(A);
+    if (rc) return rc;
+    EDX_REQUIRE(nnz_off && nval && vbits, "edx_pack_count: output pointers missing");
+    cudaStream_t st = as_stream(stream);
+    const int64_t n = A->nrows;
+    size_t temp = 0;
+    if ((rc = pack_temp_bytes(n, A->nnz, &temp))) return rc;
+    Workspace w(d_work, work_bytes);
+    PackWs p;
+    pack_layout(w, n, A->nnz, temp, &p);
+    if (!p.temp) return fail(EDX_ERR_WORKSPACE, "edx_pack_count: workspace too small");
+    const int grid = num_sms() * 8;
+    EDX_CUDA(cudaMemsetAsync(p.cnt + n, 0, sizeof(int64_t), st));
+    k_pk_count<<<grid, 256, 0, st>>>(n, A->row_ptr, A->col, p.cnt);
+    EDX_CHECK_LAUNCH();
+    size_t tb = p.temp_bytes;
+    EDX_CUDA(cub::DeviceScan::ExclusiveSum(p.temp, tb, p.cnt, p.off_ptr, (int)(n + 1), st));
+    int64_t m = 0;
+    EDX_CUDA(cudaMemcpyAsync(&m, p.off_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    EDX_CUDA(cudaStreamSynchronize(st));
+    k_pk_split<<<grid, 256, 0, st>>>(n, A->row_ptr, A->col, reinterpret_cast<const double2*>(A->val), p.off_ptr,
+                                     p.diag, p.re0, p.im0);
+    EDX_CHECK_LAUNCH();
+    int count = 0;
+    if (m > 0) {
+        // lexicographic (re, im): stable sort by im, then stable sort by re
+        tb = p.temp_bytes;
+        EDX_CUDA(cub::DeviceRadixSort::SortPairs(p.temp, tb, p.im0, p.im1, p.re0, p.re1, (int)m, 0, 64, st));
+        tb = p.temp_bytes;
+        EDX_CUDA(cub::DeviceRadixSort::SortPairs(p.temp, tb, p.re1, p.re0, p.im1, p.im0, (int)m, 0, 64, st));
+        k_pk_flags<<<grid, 256, 0, st>>>(m, p.re0, p.im0, p.flag);
+        EDX_CHECK_LAUNCH();
+        tb = p.temp_bytes;
+        EDX_CUDA(cub::DeviceScan::ExclusiveSum(p.temp, tb, p.flag, p.pos, (int)m, st));
+        k_pk_table<<<grid, 256, 0, st>>>(m, p.re0, p.im0, p.flag, p.pos, p.tre, p.tim, p.count);
+        EDX_CHECK_LAUNCH();
+        EDX_CUDA(cudaMemcpyAsync(&count, p.count, sizeof(int), cudaMemcpyDeviceToHost, st));
+        EDX_CUDA(cudaStreamSynchronize(st));
+    } else {
+        EDX_CUDA(cudaMemsetAsync(p.count, 0, sizeof(int), st));
+    }
+    const int vb = value_bits(A->ncols);
+    const int64_t cap = std::min<int64_t>(EDX_PACK_VALUES_MAX, (int64_t)1 << vb);
+    if (count > cap)
+        return fail(EDX_ERR_OVERFLOW, "edx_pack_count: %d distinct off-diagonal values, at most %lld can be packed",
+                    count, (long long)cap);
+    *nnz_off = m;
+    *nval = count;
+    *vbits = vb;
+    return EDX_OK;
+}
+
+extern "C" int edx_pack_fill(const edx_csr* A, edx_packed* P, void* d_work, size_t work_bytes, void* stream) {
+    int rc = check_square(A);
+    if (rc) return rc;
+    EDX_REQUIRE(P && P->row_ptr && P->diag && (P->nnz == 0 || (P->ent && P->vals && P->nval >= 1)),
+                "edx_pack_fill: output arrays missing");
+    cudaStream_t st = as_stream(stream);
+    const int64_t n = A->nrows;
+    size_t temp = 0;
+    if ((rc = pack_temp_bytes(n, A->nnz, &temp))) return rc;
+    Workspace w(d_work, work_bytes);
+    PackWs p;
+    pack_layout(w, n, A->nnz, temp, &p);
+    if (!p.temp) return fail(EDX_ERR_WORKSPACE, "edx_pack_fill: workspace too small");
+    int64_t m = 0;
+    int count = 0;
+    EDX_CUDA(cudaMemcpyAsync(&m, p.off_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    EDX_CUDA(cudaMemcpyAsync(&count, p.count, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EDX_CUDA(cudaStreamSynchronize(st));
+    EDX_REQUIRE(m == P->nnz && count == P->nval && P->vbits == value_bits(A->ncols),
+                "edx_pack_fill: sizes differ from the count pass");
+    P->nrows = n;
+    EDX_CUDA(cudaMemcpyAsync(const_cast<int64_t*>(P->row_ptr), p.off_ptr, sizeof(int64_t) * (size_t)(n + 1),
+                             cudaMemcpyDeviceToDevice, st));
+    EDX_CUDA(cudaMemcpyAsync(const_cast<double*>(P->diag), p.diag, sizeof(double2) * (size_t)n,
+                             cudaMemcpyDeviceToDevice, st));
+    if (m > 0) {
+        k_pk_vals<<<(count + 127) / 128, 128, 0, st>>>(count, p.tre, p.tim,
+                                                       reinterpret_cast<double2*>(const_cast<double*>(P->vals)));
+        EDX_CHECK_LAUNCH();
+        k_pk_fill<<<num_sms() * 8, 256, 0, st>>>(n, A->row_ptr, A->col, reinterpret_cast<const double2*>(A->val),
+                                                 p.off_ptr, p.tre, p.tim, count, P->vbits,
+                                                 const_cast<uint32_t*>(P->ent));
+        EDX_CHECK_LAUNCH();
+    }
+    return EDX_OK;
+}

@@ -178,4 +178,115 @@ __device__ __forceinline__ void row_times_x_tiles(int64_t start, int64_t end, co
     }
 }
 
+// Streaming loads of packed entry words (read once per product).
+__device__ __forceinline__ uint4 ld_stream4(const uint32_t* p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p), "l"(evict_first_policy()));
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_stream1(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+                 : "=r"(v)
+                 : "l"(p), "l"(evict_first_policy()));
+    return v;
+}
+
+// Off-diagonal part of row r of a packed matrix (word = column << vbits | value index; values
+// in the shared-memory table `tab`) times TG column tiles of X.  Same lane layout and result
+// as row_times_x_tiles.  With one slot per warp (KW = 32) every lane walks the same entries,
+// four words per 16-byte broadcast load, so an entry costs one table read and no shuffles.
+// With several slots, slot s takes entries start + s, start + s + SLOTS, ...; one load
+// instruction fetches adjacent words for all slots.
+template <int KW, int TG>
+__device__ __forceinline__ void row_times_x_packed(int64_t start, int64_t end, const uint32_t* __restrict__ ent,
+                                                   int vbits, const double2* tab, const double2* __restrict__ X,
+                                                   int64_t ldx_, int col0, int k, double2* acc) {
+    constexpr int SLOTS = Slots<KW>::N;
+    const int lane = threadIdx.x & 31;
+    const int slot = lane / KW;
+    const int c = lane % KW;
+    const bool slot_ok = slot < SLOTS;
+    const uint32_t vmask = (1u << vbits) - 1u;
+    bool colok[TG];
+#pragma unroll
+    for (int g = 0; g < TG; ++g) {
+        colok[g] = slot_ok && (col0 + g * KW + c < k);
+        acc[g] = make_double2(0.0, 0.0);
+    }
+    if (SLOTS == 1) {
+        auto one = [&](uint32_t w) {
+            const double2 v = tab[w & vmask];
+            const int64_t cc = (int64_t)(w >> vbits);
+#pragma unroll
+            for (int g = 0; g < TG; ++g)
+                if (colok[g]) acc[g] = fma_c(v, ldx(X + cc * ldx_ + col0 + g * KW + c), acc[g]);
+        };
+        int64_t j = start;
+        for (; j < end && (j & 3); ++j) one(ld_stream1(ent + j));
+        for (; j + 4 <= end; j += 4) {
+            const uint4 w4 = ld_stream4(ent + j);
+            const uint32_t w[4] = {w4.x, w4.y, w4.z, w4.w};
+            double2 v[4], xs[4][TG];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                v[u] = tab[w[u] & vmask];
+                const int64_t cc = (int64_t)(w[u] >> vbits);
+#pragma unroll
+                for (int g = 0; g < TG; ++g)
+                    xs[u][g] = colok[g] ? ldx(X + cc * ldx_ + col0 + g * KW + c) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int g = 0; g < TG; ++g) acc[g] = fma_c(v[u], xs[u][g], acc[g]);
+        }
+        for (; j < end; ++j) one(ld_stream1(ent + j));
+    } else {
+        constexpr int U = 4;
+        for (int64_t base = start; base < end; base += (int64_t)SLOTS * U) {
+            uint32_t w[U];
+            bool ok[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t j = base + (int64_t)u * SLOTS + slot;
+                ok[u] = slot_ok && j < end;
+                w[u] = ok[u] ? ld_stream1(ent + j) : 0u;
+            }
+            double2 v[U], xs[U][TG];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                v[u] = ok[u] ? tab[w[u] & vmask] : make_double2(0.0, 0.0);
+                const int64_t cc = (int64_t)(w[u] >> vbits);
+#pragma unroll
+                for (int g = 0; g < TG; ++g)
+                    xs[u][g] = (ok[u] && colok[g]) ? ldx(X + cc * ldx_ + col0 + g * KW + c) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int g = 0; g < TG; ++g) acc[g] = fma_c(v[u], xs[u][g], acc[g]);
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < TG; ++g) {
+        if (Slots<KW>::POW2) {
+#pragma unroll
+            for (int off = KW; off < 32; off <<= 1) acc[g] = xor_sum(acc[g], off);
+        } else {
+            double2 tot = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int s = 0; s < SLOTS; ++s) {
+                double2 o;
+                o.x = __shfl_sync(0xffffffffu, acc[g].x, s * KW + c);
+                o.y = __shfl_sync(0xffffffffu, acc[g].y, s * KW + c);
+                tot = add_c(tot, o);
+            }
+            acc[g] = tot;
+        }
+    }
+}
+
 }  // namespace edx

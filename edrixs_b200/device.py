@@ -12,7 +12,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import BuildDesc, Csr, KrylovOpts, Tiles, call
+from ._lib import BuildDesc, Csr, KrylovOpts, Packed, Tiles, call
 
 C128, C64 = _lib.EDX_C128, _lib.EDX_C64
 HAM_I, HAM_N, TRANS_I, TRANS_F = _lib.EDX_HAM_I, _lib.EDX_HAM_N, _lib.EDX_TRANS_I, _lib.EDX_TRANS_F
@@ -263,6 +263,66 @@ def tiles_for(A: CSR, basis: Basis):
 
 
 # ------------------------------------------------------------------------------------
+# packed form (edx_pack_*)
+# ------------------------------------------------------------------------------------
+
+PACK_VALUES_MAX = 2048
+
+
+@dataclass
+class PackedMatrix:
+    """Device arrays of an edx_packed matrix (see include/edx.h); keeps them alive."""
+    row_ptr: torch.Tensor   # int64 [n+1], off-diagonal entries
+    ent: torch.Tensor       # int32 [nnz] holding the uint32 words column << vbits | value index
+    vals: torch.Tensor      # complex128 [nval]
+    diag: torch.Tensor      # complex128 [n]
+    vbits: int
+
+    @property
+    def nrows(self):
+        return self.row_ptr.numel() - 1
+
+    def desc(self):
+        return Packed(self.nrows, self.ent.numel(), _ptr(self.row_ptr), _ptr(self.ent), self.vbits,
+                      self.vals.numel(), _ptr(self.vals), _ptr(self.diag))
+
+    def nbytes(self):
+        return sum(t.numel() * t.element_size() for t in (self.row_ptr, self.ent, self.vals, self.diag))
+
+    def unpack(self):
+        """(row_ptr, col, val) of the off-diagonal entries, for checks."""
+        w = self.ent.to(torch.int64) & 0xFFFFFFFF
+        return self.row_ptr, (w >> self.vbits), self.vals[w & ((1 << self.vbits) - 1)]
+
+
+def pack(A: CSR):
+    """Packed form of the square complex128 matrix A, or None when A has more distinct
+    off-diagonal values than a 32-bit entry word can index."""
+    require_cuda()
+    d = A.desc()
+    ws = ctypes.c_size_t(0)
+    call("edx_pack_workspace", ctypes.byref(d), ctypes.byref(ws))
+    w = _work(ws.value)
+    nnz, nval, vbits = ctypes.c_int64(0), ctypes.c_int(0), ctypes.c_int(0)
+    st = _stream()
+    try:
+        call("edx_pack_count", ctypes.byref(d), ctypes.byref(nnz), ctypes.byref(nval), ctypes.byref(vbits),
+             _ptr(w), ws.value, st)
+    except _lib.EdxError as e:
+        if e.code == 5:  # EDX_ERR_OVERFLOW: too many distinct values
+            return None
+        raise
+    n = A.nrows
+    P = PackedMatrix(torch.empty(n + 1, dtype=torch.int64, device="cuda"),
+                     torch.empty(max(nnz.value, 1), dtype=torch.int32, device="cuda")[:nnz.value],
+                     torch.empty(max(nval.value, 1), dtype=torch.complex128, device="cuda")[:nval.value],
+                     torch.empty(n, dtype=torch.complex128, device="cuda"), vbits.value)
+    t = P.desc()
+    call("edx_pack_fill", ctypes.byref(d), ctypes.byref(t), _ptr(w), ws.value, st)
+    return P
+
+
+# ------------------------------------------------------------------------------------
 # products and solvers
 # ------------------------------------------------------------------------------------
 
@@ -347,6 +407,10 @@ def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, s
             tdesc = apply["layout"].desc()
             opts.apply_layout = ctypes.pointer(tdesc)
             keep += [tdesc]
+        if apply.get("packed") is not None:
+            pdesc = apply["packed"].desc()
+            opts.apply_packed = ctypes.pointer(pdesc)
+            keep += [pdesc]
     ms = ctypes.c_double(0.0)
     nl = ctypes.c_int(0)
     if timing:

@@ -48,27 +48,33 @@ class RixsProblem:
     gs_e: np.ndarray
     gs_v: torch.Tensor                       # (n_i, ngs) complex128
     meta: dict = field(default_factory=dict)
-    tiles: dict = field(default_factory=dict)  # "hf" / "hn" -> device.TiledLayout of that matrix
+    tiles: dict = field(default_factory=dict)   # "hf" / "hn" -> device.TiledLayout of that matrix
+    packed: dict = field(default_factory=dict)  # "hf" / "hn" -> device.PackedMatrix of that matrix
 
     def nbytes(self):
         b = self.Hn.nbytes() + self.Hf.nbytes() + sum(D.nbytes() for D in self.Din + self.Dout)
         if self.Hn.val64 is not None:
             b += self.Hn.nnz * 8
         b += sum(L.nbytes() for L in self.tiles.values())
+        b += sum(M.nbytes() for M in self.packed.values())
         return b + self.gs_v.numel() * 16
 
 
-def _apply_args(cfg, layout, k, c64):
-    """Launch arguments of one Krylov call: the autotuner's choice, else the tiled product for
-    a wide block (k >= 32) when a layout exists, else libedx's defaults."""
+def _apply_args(cfg, layout, packed, c64):
+    """Launch arguments of one Krylov call: the autotuner's choice, else the packed product
+    when a packed form exists, else libedx's defaults."""
     if cfg is not None:
         if cfg.get("tiled"):
             if layout is None:
                 raise ValueError("the tuned launch shape needs the tiled layout")
             return dict(layout=layout)
+        if cfg.get("packed"):
+            if packed is None:
+                raise ValueError("the tuned launch shape needs the packed form")
+            return dict(cfg, packed=packed)
         return cfg
-    if layout is not None and not c64 and k >= 32:
-        return dict(layout=layout)
+    if packed is not None and not c64:
+        return dict(packed=packed)
     return None
 
 
@@ -92,10 +98,12 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     K_hf = npout * k_hn * n_om if final_block is None else int(final_block)
     if autotune:
         from . import tune
-        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64, layout=P.tiles.get("hn"))
-        P.meta[("apply", "hf", K_hf, c64)] = tune.tune_apply(P.Hf, K_hf, c64=c64, layout=P.tiles.get("hf"))
-    cfg_hn = _apply_args(P.meta.get(("apply", "hn", k_hn, c64)), P.tiles.get("hn"), k_hn, c64)
-    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64)), P.tiles.get("hf"), K_hf, c64)
+        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64, layout=P.tiles.get("hn"),
+                                                             packed=P.packed.get("hn"))
+        P.meta[("apply", "hf", K_hf, c64)] = tune.tune_apply(P.Hf, K_hf, c64=c64, layout=P.tiles.get("hf"),
+                                                             packed=P.packed.get("hf"))
+    cfg_hn = _apply_args(P.meta.get(("apply", "hn", k_hn, c64)), P.tiles.get("hn"), P.packed.get("hn"), c64)
+    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64)), P.tiles.get("hf"), P.packed.get("hf"), c64)
     gam_c = np.broadcast_to(np.asarray(gamma_c, dtype=np.float64), (n_om,))
     dev = P.gs_v.device
     # 1. seeds (n_n, npin*ngs), column c = p_in*ngs + g
@@ -114,9 +122,10 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     iters = r.shift_iters.view(k, n_om).cpu().numpy()
     resid = r.shift_res.view(k, n_om).cpu().numpy()
     it_n = r.apply_launches
-    # libedx launches on H_n: 4 setup + per iteration (apply, orth, shift step, scale, projections)
+    # libedx launches on H_n: 4 setup + the first projections, then per iteration apply, orth,
+    # shift step and per emission operator a projection and its column scaling
     stats = dict(hn_iterations=it_n, hn_apply_ms=r.apply_ms, hn_nnz=P.Hn.nnz, hn_rows=P.Hn.nrows, k_hn=k,
-                 launches=len(P.Din) + 4 + npout + it_n * (4 + npout))
+                 launches=len(P.Din) + 4 + npout + it_n * (3 + 2 * npout))
     Y = r.shift_y.view(k, n_om, -1)[:, :, :m]                     # (k, n_om, m)
     # phi[p_out][c, w, :] = sum_i Y[c, w, i] * (D_out^+ v_i)[:]
     phis = []
@@ -142,9 +151,11 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
         A[s:e], B[s:e], NRM[s:e], NEFF[s:e] = rf.alpha, rf.beta, rf.norm, rf.neff
         hf_ms += rf.apply_ms or 0.0
         hf_it += rf.apply_launches
-        stats["launches"] += 2 + 3 * rf.apply_launches
+        stats["launches"] += 2 + 2 * rf.apply_launches  # norm, start; apply + orth per step
     stats.update(hf_apply_ms=hf_ms if timing else None, hf_iterations=hf_it, hf_nnz=P.Hf.nnz, hf_rows=P.Hf.nrows,
-                 k_hf=blk, hf_tiled=bool(cfg_hf and cfg_hf.get("layout") is not None))
+                 k_hf=blk, hf_tiled=bool(cfg_hf and cfg_hf.get("layout") is not None),
+                 hf_packed=bool(cfg_hf and cfg_hf.get("packed") is not None),
+                 hn_packed=bool(cfg_hn and cfg_hn.get("packed") is not None))
     del V0
     # 5. continued fractions; column order (p_out, p_in, g, w)
     e0 = np.tile(np.repeat(np.tile(P.gs_e, npin), n_om), npout)

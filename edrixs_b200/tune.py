@@ -32,16 +32,15 @@ def candidates(k):
         for tg in tiles:
             for th, bps in shapes:
                 for ch in (0, 1):
-                    for pf in (0, 1):
-                        out.append(dict(col_group=kw, tiles=tg, threads=th, blocks_per_sm=bps, chunked=ch,
-                                        prefetch=pf))
+                    out.append(dict(col_group=kw, tiles=tg, threads=th, blocks_per_sm=bps, chunked=ch))
     return out
 
 
-def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None):
-    """Fastest launch shape for k columns on A.  With a tiled layout of A (complex128 only)
-    the tiled product is timed too and reported as {"tiled": 1}."""
-    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64), layout is not None)
+def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None, packed=None):
+    """Fastest launch shape for k columns on A.  With a tiled layout or a packed form of A
+    (complex128 only) those products are timed too; the result then carries "tiled": 1 or
+    "packed": 1."""
+    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64), layout is not None, packed is not None)
     if key in _cache:
         return _cache[key]
     g = torch.Generator(device=A.val.device)
@@ -50,10 +49,17 @@ def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None)
     best, best_t = None, float("inf")
     results = []
     cands = candidates(k)
+    if packed is not None and not c64:
+        cands = cands + [dict(c, packed=1) for c in candidates(k)]
     if layout is not None and not c64:
         cands = [dict(tiled=1)] + cands
     for cfg in cands:
-        args = dict(layout=layout) if cfg.get("tiled") else cfg
+        if cfg.get("tiled"):
+            args = dict(layout=layout)
+        elif cfg.get("packed"):
+            args = dict(cfg, packed=packed)
+        else:
+            args = cfg
         r = device.krylov(A, V0, steps, c64=c64, timing=True, apply=args)
         t = r.apply_ms / max(r.apply_launches, 1)
         results.append((t, cfg))

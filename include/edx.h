@@ -181,6 +181,38 @@ int edx_tiles_count(const edx_csr* A, int32_t ntile_r, const int32_t* d_tile_r, 
 int edx_tiles_fill(const edx_csr* A, edx_tiles* T, void* d_work, size_t work_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------- */
+/* Packed form of a square matrix (no counterpart in the reference)                    */
+/* ---------------------------------------------------------------------------------- */
+
+/* A Hamiltonian built from a few hundred hopping and Coulomb terms has only a few hundred
+ * distinct off-diagonal values (for example 418 in the 11.2 M entries of a 184,756-state
+ * impurity model).  The packed form keeps the diagonal as a dense complex128 vector and
+ * stores every off-diagonal entry as one 32-bit word:
+ *   ent = column << vbits | index into vals (the distinct values, bit-exact copies),
+ * with vbits = 32 - (bits of ncols-1).  Rows keep the CSR's column order.  The form exists
+ * when nval <= min(2^vbits, EDX_PACK_VALUES_MAX). */
+#define EDX_PACK_VALUES_MAX 2048
+typedef struct edx_packed {
+    int64_t nrows;
+    int64_t nnz;               /* off-diagonal entries */
+    const int64_t* row_ptr;    /* device int64[nrows+1] */
+    const uint32_t* ent;       /* device uint32[nnz] */
+    int vbits;
+    int nval;
+    const double* vals;        /* device complex128[nval] */
+    const double* diag;        /* device complex128[nrows]; zero where the CSR has no diagonal */
+} edx_packed;
+
+int edx_pack_workspace(const edx_csr* A, size_t* bytes);
+/* Pass 1: *nnz_off, *nval, *vbits of complex128 square A.  EDX_ERR_OVERFLOW when A has too
+ * many distinct off-diagonal values to pack.  Synchronises `stream`. */
+int edx_pack_count(const edx_csr* A, int64_t* nnz_off, int* nval, int* vbits, void* d_work,
+                   size_t work_bytes, void* stream);
+/* Pass 2: P->nnz, nval, vbits from pass 1 and its four arrays allocated by the caller;
+ * d_work must still hold what pass 1 left in it. */
+int edx_pack_fill(const edx_csr* A, edx_packed* P, void* d_work, size_t work_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------------- */
 /* Lanczos / Krylov                                                                     */
 /* ---------------------------------------------------------------------------------- */
 
@@ -229,6 +261,10 @@ typedef struct edx_krylov_opts {
      * vectors is staged in shared memory once and used for all rows of the row tile.
      * complex128 matrices only; the launch-shape fields above are then ignored. */
     const edx_tiles* apply_layout;
+    /* packed form of the same matrix (edx_pack_fill), or NULL.  With it the product reads
+     * one 32-bit word per off-diagonal entry and the value from a table in shared memory,
+     * with the launch-shape fields above (the tiled layout takes precedence). */
+    const edx_packed* apply_packed;
 } edx_krylov_opts;
 
 /* k independent Lanczos recurrences of build_krylov_mp (src/lanczos.f90:210-303), run

@@ -53,11 +53,10 @@ def parse():
 
 def kernel_case(args):
     """The apply kernels on this workload's matrices at the launch shapes the autotuner picks
-    for the timed steps (a few GB on the device): one Lanczos step of H_n on the 6 seed
-    columns, one of H_f on 256 final-state columns (each column group of 64 sweeps the same
-    rows and x columns as in the 768-column timed launches, one third as many groups), and
-    one SpMV of the one-RHS MINRES.  Each Krylov call of two steps launches the apply
-    kernel twice."""
+    (a few GB on the device): two Lanczos steps of H_n on the 6 seed columns and of H_f on 256
+    final-state columns (each column group of 64 sweeps the same rows and x columns as in the
+    768-column timed launches, one third as many groups), first with the CSR products, then
+    with the packed ones, and one SpMV of the one-RHS MINRES."""
     import torch
     from edrixs_b200 import device
     m, t = workload_terms(args.nbath, args.nelec)
@@ -71,6 +70,10 @@ def kernel_case(args):
     device.krylov(Hn, V, 2, apply=dict(col_group=6, tiles=1, threads=1024, blocks_per_sm=1, chunked=0))
     W = torch.randn((Hf.nrows, 256), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
     device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1, chunked=0))
+    # the packed products at the shapes the autotuner picks for them
+    Pn, Pf = device.pack(Hn), device.pack(Hf)
+    device.krylov(Hn, V, 2, apply=dict(col_group=6, tiles=1, threads=1024, blocks_per_sm=2, chunked=1, packed=Pn))
+    device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=256, blocks_per_sm=4, chunked=0, packed=Pf))
     b = torch.randn(Hn.nrows, dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
     device.minres(Hn, b, 1e-300, 1, alpha=-1.0, sigma=40 + 0.6j)
     torch.cuda.synchronize()

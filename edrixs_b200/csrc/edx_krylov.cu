@@ -176,7 +176,7 @@ struct PackedView {
 };
 
 template <int KW, int TG, int NT>
-__global__ void __launch_bounds__(NT) k_lanczos_apply_packed(int64_t n, PackedView M, const double2* __restrict__ Vc,
+__global__ void __launch_bounds__(NT, 1024 / NT) k_lanczos_apply_packed(int64_t n, PackedView M, const double2* __restrict__ Vc,
                                                              double2* __restrict__ Vp, KrylovState S, int it,
                                                              int chunked) {
     constexpr int NW = NT / 32;

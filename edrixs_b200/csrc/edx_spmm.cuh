@@ -246,6 +246,13 @@ __device__ __forceinline__ void row_times_x_packed(int64_t start, int64_t end, c
         for (; j < end; ++j) one(ld_stream1(ent + j));
     } else {
         constexpr int U = 4;
+        // words of the next U groups load while this batch's gathers run
+        uint32_t nw[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t j = start + (int64_t)u * SLOTS + slot;
+            nw[u] = (slot_ok && j < end) ? ld_stream1(ent + j) : 0u;
+        }
         for (int64_t base = start; base < end; base += (int64_t)SLOTS * U) {
             uint32_t w[U];
             bool ok[U];
@@ -253,7 +260,9 @@ __device__ __forceinline__ void row_times_x_packed(int64_t start, int64_t end, c
             for (int u = 0; u < U; ++u) {
                 const int64_t j = base + (int64_t)u * SLOTS + slot;
                 ok[u] = slot_ok && j < end;
-                w[u] = ok[u] ? ld_stream1(ent + j) : 0u;
+                w[u] = nw[u];
+                const int64_t jn = j + (int64_t)SLOTS * U;
+                nw[u] = (slot_ok && jn < end) ? ld_stream1(ent + jn) : 0u;
             }
             double2 v[U], xs[U][TG];
 #pragma unroll

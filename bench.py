@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-packed", action="store_true", help="no packed forms of H_n, H_f (CSR products only)")
     ap.add_argument("--tiles", action="store_true", help="also offer the tiled layout of H_f to the autotuner")
-    ap.add_argument("--kernel-case", choices=["apply", "hf-shapes"], default=None,
+    ap.add_argument("--kernel-case", choices=["apply", "hf-shapes", "all"], default=None,
                     help="run only a small profiling case of the dominant kernels (for ncu)")
     return ap.parse_args()
 
@@ -97,6 +97,55 @@ def kernel_case_hf_shapes(args):
                                                chunked=chunked))
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": "hf-shapes", "nnz_Hf": Hf.nnz}))
+
+
+def kernel_case_all(args):
+    """Every libedx kernel once or twice on this workload's matrices (for a per-kernel DRAM
+    summary): Fock unranking (the 2.7 M-state C(24,12) sector too), the count/fill builds of
+    H_f, H_n, D_in and D_out, the one-column SpMV and the 6-column SpMM, two Lanczos steps
+    on H_n (6 columns, with shifts and projections) and H_f (256 columns) on the CSR, packed
+    and tiled forms with their builders, two MINRES steps on H_n, the continued fraction
+    (768 pole sets x 2000 points) and the density matrix."""
+    import torch
+    from edrixs_b200 import device
+    m, t = workload_terms(args.nbath, args.nelec)
+    nv, N = m.nv, args.nelec
+    device.fock_unrank(24, 12)
+    bi, bn = device.fock_unrank(nv, N), device.fock_unrank(nv, N + 1)
+    Hf = device.build_csr(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
+    Hn = device.build_csr(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    Din = device.build_csr(device.TRANS_I, bn, t["din"][0], right=bi, num_val_orbs=nv, num_core_orbs=6)
+    Dout = device.build_csr(device.TRANS_F, bi, t["dout"][0], right=bn, num_val_orbs=nv, num_core_orbs=6)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+
+    def crand(*shape):
+        return torch.randn(shape, dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+
+    x1 = crand(Hn.nrows)
+    device.spmm(Hn, x1)
+    V = crand(Hn.nrows, 6)
+    device.spmm(Dout, V)
+    seeds = device.spmm(Din, crand(Hf.nrows, 6))
+    shifts = (np.repeat(np.arange(6), 4), np.tile(np.array([40 + 0.6j, 41 + 0.6j, 42 + 0.6j, 43 + 0.6j]), 6))
+    device.krylov(Hn, seeds, 2, proj=[Dout], shifts=shifts)
+    Pn, Pf = device.pack(Hn), device.pack(Hf)
+    device.krylov(Hn, V, 2, apply=dict(col_group=6, threads=1024, blocks_per_sm=1, packed=Pn))
+    W = crand(Hf.nrows, 256)
+    device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1))
+    device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1, packed=Pf))
+    L = device.tiles_for(Hf, bi)
+    device.krylov(Hf, W, 2, apply=dict(layout=L))
+    device.minres(Hn, x1, 1e-300, 2, alpha=-1.0, sigma=40 + 0.6j)
+    K, nk = 768, 150
+    al = 20 * torch.rand((K, nk), dtype=torch.float64, device="cuda", generator=g)
+    be = torch.rand((K, nk), dtype=torch.float64, device="cuda", generator=g)
+    device.cf_spectrum(torch.full((K,), nk, dtype=torch.int32, device="cuda"), al, be, np.zeros(K), np.ones(K),
+                       np.ones(K), np.linspace(-0.5, 12.0, 2000), 0.1)
+    device.denmat(bi, nv, crand(Hf.nrows, 3))
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": "all", "nnz_Hn": Hn.nnz, "nnz_Hf": Hf.nnz, "nnz_Din": Din.nnz,
+                      "nnz_Dout": Dout.nnz}))
 
 
 def load_peaks():
@@ -244,6 +293,35 @@ def cpu_sample(args, t, gs, omega, iters_minres, minres_its=60, krylov_steps=60)
 # ------------------------------------------------------------------------------------
 # arms
 # ------------------------------------------------------------------------------------
+
+def spmv_roofline(P, peak):
+    """The one-column complex128 CSR SpMV (edx_spmm, the product of the reference's
+    matvec_csr) on H_n, timed with CUDA events over 20 launches: the HBM-bound case of the
+    SpMV/SpMM.  Algorithmic bytes: nnz*(16+4) + (n+1)*8 + 2*n*16 (A, x, y once)."""
+    import torch
+    from edrixs_b200 import device
+    A = P.Hn
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    x = torch.randn(A.nrows, dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    y = torch.zeros_like(x)
+    for _ in range(3):
+        device.spmm(A, x, y)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        device.spmm(A, x, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    byts = A.nnz * 20 + (A.nrows + 1) * 8 + 2 * A.nrows * 16
+    ach = byts / (ms / 1e3) / 1e9
+    return dict(kernel="k_spmm<1> on H_n (one column, complex128 CSR)", bound="hbm", achieved=round(ach, 1),
+                peak=peak, unit="GB/s", frac=round(ach / peak, 4), bytes_per_launch=int(byts),
+                avg_launch_us=round(ms * 1e3, 2), launches=reps)
+
 
 def _cf_np(alpha, beta, norm, neff, z):
     """norm / (z - a0 - b1^2 / (z - a1 - ...)) on the host (the continued fraction of
@@ -442,7 +520,7 @@ def run_ours(args):
     hn_kernel = "k_lanczos_apply_packed" if st.get("hn_packed") else "k_lanczos_apply"
     dom_name = f"{hf_kernel} on H_f (768 columns)" if dom is r_hf else f"{hn_kernel} on H_n (6 columns)"
 
-    extra = {}
+    extra = {"spmv_roofline": spmv_roofline(P, peak)}
     if rank == 0 and not args.no_plain:
         # the plain FP64 one-RHS GPU path (the reference's algorithm per point) on one omega
         # for all 12 (pol pair, gs) points, and its spectral error vs the batched result
@@ -539,6 +617,8 @@ if __name__ == "__main__":
     a = parse()
     if a.kernel_case == "hf-shapes":
         kernel_case_hf_shapes(a)
+    elif a.kernel_case == "all":
+        kernel_case_all(a)
     elif a.kernel_case:
         kernel_case(a)
     elif a.impl == "reference":

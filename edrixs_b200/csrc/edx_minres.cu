@@ -90,12 +90,15 @@ __global__ void __launch_bounds__(MT) k_mr_apply(int64_t n, const int64_t* __res
         part[2 * blockIdx.x + 1] = si;
     }
     if (mr_last(&S->ticket[0])) {
+        // every thread adds a fixed subset of the block partials, then a fixed-order tree
+        double ar = 0.0, ai = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += MT) {
+            ar += __ldcg(part + 2 * b);
+            ai += __ldcg(part + 2 * b + 1);
+        }
+        ar = block_sum(ar);
+        ai = block_sum(ai);
         if (threadIdx.x == 0) {
-            double ar = 0.0, ai = 0.0;
-            for (int b = 0; b < (int)gridDim.x; ++b) {
-                ar += __ldcg(part + 2 * b);
-                ai += __ldcg(part + 2 * b + 1);
-            }
             S->alpha = make_double2(ar, ai);
             S->ticket[0] = 0u;
         }
@@ -118,9 +121,10 @@ __global__ void __launch_bounds__(MT) k_mr_orth(int64_t n, const double2* __rest
     double s = block_sum(p);
     if (threadIdx.x == 0) part[blockIdx.x] = s;
     if (mr_last(&S->ticket[1])) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += MT) t += __ldcg(part + b);
+        t = block_sum(t);
         if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(part + b);
             const double beta1 = sqrt(t);
             MinresState q = *S;
             const double2 alpha = q.alpha;

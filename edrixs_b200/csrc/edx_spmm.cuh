@@ -90,12 +90,14 @@ __device__ __forceinline__ void row_times_x_tiles(int64_t start, int64_t end, co
         acc[g] = zero_c<AT>();
     }
     if (KW == 1) {
-        // each lane owns its own entries; U rounds of 32 per pass
-        for (int64_t base = start; base < end; base += 32 * U) {
-            int cc[U];
-            AT vv[U];
+        // each lane owns its own entries; U1 rounds of 32 per pass, so a typical row
+        // issues all its loads at once
+        constexpr int U1 = 4;
+        for (int64_t base = start; base < end; base += 32 * U1) {
+            int cc[U1];
+            AT vv[U1];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
+            for (int u = 0; u < U1; ++u) {
                 const int64_t j = base + u * 32 + lane;
                 cc[u] = 0;
                 vv[u] = zero_c<AT>();
@@ -104,9 +106,9 @@ __device__ __forceinline__ void row_times_x_tiles(int64_t start, int64_t end, co
                     vv[u] = to_acc(ld_stream(val + j), AT());
                 }
             }
-            AT xs[U][TG];
+            AT xs[U1][TG];
 #pragma unroll
-            for (int u = 0; u < U; ++u)
+            for (int u = 0; u < U1; ++u)
 #pragma unroll
                 for (int g = 0; g < TG; ++g) {
                     xs[u][g] = zero_c<AT>();
@@ -114,7 +116,7 @@ __device__ __forceinline__ void row_times_x_tiles(int64_t start, int64_t end, co
                         xs[u][g] = to_acc(ldx(X + (int64_t)cc[u] * ldx_ + col0 + g), AT());
                 }
 #pragma unroll
-            for (int u = 0; u < U; ++u)
+            for (int u = 0; u < U1; ++u)
 #pragma unroll
                 for (int g = 0; g < TG; ++g) acc[g] = fma_c(vv[u], xs[u][g], acc[g]);
         }

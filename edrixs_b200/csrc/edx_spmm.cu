@@ -11,25 +11,65 @@
 
 namespace edx {
 
+// Short rows (a transition operator has ~10 entries per row): each slot of the warp owns a
+// row of its own and walks its entries, U at a time, with the slot's KW lanes reading the
+// same entry (a broadcast) and gathering their own columns of X.  No cross-slot reduction.
 template <int KW, class VT, class XT>
+__device__ __forceinline__ void row_times_x_slot(int64_t start, int64_t end, const int32_t* __restrict__ col,
+                                                 const VT* __restrict__ val, const XT* __restrict__ X,
+                                                 int64_t ldx_, int gc, bool colok, typename Acc<VT, XT>::T& acc) {
+    using AT = typename Acc<VT, XT>::T;
+    constexpr int U = 4;
+    acc = zero_c<AT>();
+    for (int64_t base = start; base < end; base += U) {
+        int cc[U];
+        AT vv[U], xs[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool ok = base + u < end;
+            cc[u] = ok ? __ldg(col + base + u) : 0;
+            vv[u] = ok ? to_acc(__ldg(val + base + u), AT()) : zero_c<AT>();
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            xs[u] = (base + u < end && colok) ? to_acc(ldx(X + (int64_t)cc[u] * ldx_ + gc), AT()) : zero_c<AT>();
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc = fma_c(vv[u], xs[u], acc);
+    }
+}
+
+template <int KW, class VT, class XT, bool ROWSLOT>
 __global__ void __launch_bounds__(256) k_spmm(int64_t nrows, const int64_t* __restrict__ row_ptr,
                                               const int32_t* __restrict__ col, const VT* __restrict__ val,
                                               int k, const XT* __restrict__ X, int64_t ldx_, XT* __restrict__ Y,
                                               int64_t ldy, int64_t ycs, double2 alpha, double2 sigma,
                                               double2 beta, int has_sigma, int has_beta) {
     using AT = typename Acc<VT, XT>::T;
+    constexpr int SLOTS = Slots<KW>::N;
     const int lane = threadIdx.x & 31;
     const int c = lane % KW;
+    const int slot = lane / KW;
     const int gc = blockIdx.y * KW + c;
     const bool colok = gc < k;
     const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r = warp0; r < nrows; r += nw) {
-        const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
-        AT accv[1];
-        row_times_x_tiles<KW, 1, VT, XT>(s, e, col, val, X, ldx_, blockIdx.y * KW, k, accv);
-        const AT acc = accv[0];
-        if (lane < KW && colok) {
+    const int64_t rstep = ROWSLOT ? nw * SLOTS : nw;
+    for (int64_t rb = ROWSLOT ? warp0 * SLOTS : warp0; rb < nrows; rb += rstep) {
+        const int64_t r = ROWSLOT ? rb + slot : rb;
+        AT acc;
+        bool mine;
+        if (ROWSLOT) {
+            mine = slot < SLOTS && r < nrows;
+            const int64_t s = mine ? __ldg(row_ptr + r) : 0, e = mine ? __ldg(row_ptr + r + 1) : 0;
+            row_times_x_slot<KW, VT, XT>(s, e, col, val, X, ldx_, gc, colok, acc);
+        } else {
+            mine = lane < KW;
+            const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
+            AT accv[1];
+            row_times_x_tiles<KW, 1, VT, XT>(s, e, col, val, X, ldx_, blockIdx.y * KW, k, accv);
+            acc = accv[0];
+        }
+        if (mine && colok) {
             double yr = alpha.x * (double)acc.x - alpha.y * (double)acc.y;
             double yi = alpha.x * (double)acc.y + alpha.y * (double)acc.x;
             if (has_sigma) {
@@ -51,21 +91,32 @@ __global__ void __launch_bounds__(256) k_spmm(int64_t nrows, const int64_t* __re
     }
 }
 
+// rows of at most this many entries on average run one row per slot
+constexpr int64_t SHORT_ROW = 16;
+
 template <int KW, class VT, class XT>
 static int launch_spmm_t(const edx_csr* A, int k, const void* x, int64_t ldx_, void* y, int64_t ldy,
                          int64_t ycs, double2 al, double2 sg, double2 be, cudaStream_t st) {
     const int threads = 256;
-    int64_t need = (A->nrows * 32 + threads - 1) / threads;
+    const bool rowslot = KW < 32 && A->nnz <= SHORT_ROW * A->nrows;
+    const int64_t rows_per_warp = rowslot ? 32 / KW : 1;
+    int64_t need = ((A->nrows + rows_per_warp - 1) / rows_per_warp * 32 + threads - 1) / threads;
     int64_t maxb = (int64_t)num_sms() * 8;
     int64_t bx = need < maxb ? need : maxb;
     if (bx < 1) bx = 1;
     dim3 grid((unsigned)bx, (unsigned)((k + KW - 1) / KW));
     const int hs = (sg.x != 0.0 || sg.y != 0.0) ? 1 : 0;
     const int hb = (be.x != 0.0 || be.y != 0.0) ? 1 : 0;
-    k_spmm<KW, VT, XT><<<grid, threads, 0, st>>>(A->nrows, A->row_ptr, A->col,
-                                                  reinterpret_cast<const VT*>(A->val), k,
-                                                  reinterpret_cast<const XT*>(x), ldx_,
-                                                  reinterpret_cast<XT*>(y), ldy, ycs, al, sg, be, hs, hb);
+    if (rowslot)
+        k_spmm<KW, VT, XT, true><<<grid, threads, 0, st>>>(A->nrows, A->row_ptr, A->col,
+                                                            reinterpret_cast<const VT*>(A->val), k,
+                                                            reinterpret_cast<const XT*>(x), ldx_,
+                                                            reinterpret_cast<XT*>(y), ldy, ycs, al, sg, be, hs, hb);
+    else
+        k_spmm<KW, VT, XT, false><<<grid, threads, 0, st>>>(A->nrows, A->row_ptr, A->col,
+                                                             reinterpret_cast<const VT*>(A->val), k,
+                                                             reinterpret_cast<const XT*>(x), ldx_,
+                                                             reinterpret_cast<XT*>(y), ldy, ycs, al, sg, be, hs, hb);
     EDX_CHECK_LAUNCH();
     return EDX_OK;
 }

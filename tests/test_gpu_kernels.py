@@ -140,6 +140,26 @@ def test_spmm_c128(hn_pair, k):
     assert np.abs(Yt2.cpu().numpy() - want2).max() <= 1e-13 * np.abs(want2).max()
 
 
+@pytest.mark.parametrize("k", [1, 6, 8, 40])
+def test_spmm_short_rows(cuda, k):
+    """A transition operator (about 10 entries per row) takes the row-per-slot mapping."""
+    import torch
+    from edrixs_b200 import device
+    m, t = _model_terms(6, 8, seed=5)
+    fi, fn = orc.fock_full_N(m.nv, 8), orc.fock_full_N(m.nv, 9)
+    ref = orc.build_csr("trans_f", fi, t["tr_f"], fock_right=fn, num_val_orbs=m.nv, num_core_orbs=6)
+    gpu = device.build_csr(device.TRANS_F, device.basis_from_states(fi), t["tr_f"],
+                           right=device.basis_from_states(fn), num_val_orbs=m.nv, num_core_orbs=6)
+    assert ref.nnz <= 16 * ref.nrows
+    rng = np.random.default_rng(k)
+    X = rng.normal(size=(ref.ncols, k)) + 1j * rng.normal(size=(ref.ncols, k))
+    Y0 = rng.normal(size=(ref.nrows, k)) + 1j * rng.normal(size=(ref.nrows, k))
+    Yt = torch.from_numpy(Y0).cuda()
+    device.spmm(gpu, torch.from_numpy(X).cuda(), Yt, alpha=1.0, beta=1.0)
+    want = np.stack([orc.matvec(ref, X[:, c], Y0[:, c].copy()) for c in range(k)], axis=1)
+    assert np.abs(Yt.cpu().numpy() - want).max() <= 1e-13 * np.abs(want).max()
+
+
 @pytest.mark.parametrize("k", [1, 8])
 def test_spmm_c64(hn_pair, k):
     import torch

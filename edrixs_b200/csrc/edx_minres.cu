@@ -69,11 +69,7 @@ __global__ void __launch_bounds__(MT) k_mr_apply(int64_t n, const int64_t* __res
     double pr = 0.0, pi = 0.0;
     const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r = w0; r < n; r += nw) {
-        const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
-        double2 accv[1];
-        row_times_x_tiles<1, 1, VT, double2>(s, e, col, val, v, 1, 0, 1, accv);
-        const double2 acc = accv[0];
+    spmv_rows<VT, double2>(w0, n, nw, row_ptr, col, val, v, 1, 0, [&](int64_t r, double2 acc) {
         if (lane == 0) {
             double2 vr = v[r];
             double2 t = cmul(aop, acc);
@@ -82,7 +78,7 @@ __global__ void __launch_bounds__(MT) k_mr_apply(int64_t n, const int64_t* __res
             pr += vr.x * t.x + vr.y * t.y;
             pi += vr.x * t.y - vr.y * t.x;
         }
-    }
+    });
     double sr = block_sum(pr);
     double si = block_sum(pi);
     if (threadIdx.x == 0) {
@@ -335,7 +331,14 @@ extern "C" int edx_minres(const edx_csr* A, double alpha_re, double alpha_im, do
     k_mr_init2<<<1, 32, 0, st>>>(g, part, S, tol, maxit);
     EDX_CHECK_LAUNCH();
     const double2 aop = make_double2(alpha_re, alpha_im), sop = make_double2(sigma_re, sigma_im);
-    const int ga = (int)std::min<int64_t>((n * 32 + MT - 1) / MT, (int64_t)num_sms() * 8);
+    // the SpMV runs as one wave of resident blocks (at most 8 per SM: the partials buffer)
+    int res = 4;
+    if (A->val_type == EDX_C128)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, k_mr_apply<double2>, MT, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, k_mr_apply<float2>, MT, 0);
+    res = std::max(1, std::min(res, 8));
+    const int ga = (int)std::min<int64_t>((n * 32 + MT - 1) / MT, (int64_t)num_sms() * res);
     const int poll = 8;
     for (int it = 0; it < maxit; ++it) {
         k_mr_scale<<<g, MT, 0, st>>>(n, vc, S, it);

@@ -53,6 +53,31 @@ __global__ void __launch_bounds__(256) k_spmm(int64_t nrows, const int64_t* __re
     const bool colok = gc < k;
     const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    auto store = [&](int64_t r, AT acc) {
+        double yr = alpha.x * (double)acc.x - alpha.y * (double)acc.y;
+        double yi = alpha.x * (double)acc.y + alpha.y * (double)acc.x;
+        if (has_sigma) {
+            XT xv = X[r * ldx_ + gc];
+            yr += sigma.x * (double)xv.x - sigma.y * (double)xv.y;
+            yi += sigma.x * (double)xv.y + sigma.y * (double)xv.x;
+        }
+        XT* yp = Y + r * ldy + (int64_t)gc * ycs;
+        if (has_beta) {
+            XT yv = *yp;
+            yr += beta.x * (double)yv.x - beta.y * (double)yv.y;
+            yi += beta.x * (double)yv.y + beta.y * (double)yv.x;
+        }
+        XT out;
+        out.x = yr;
+        out.y = yi;
+        *yp = out;
+    };
+    if (KW == 1 && !ROWSLOT) {  // one column, long rows: the next row loads during this one
+        spmv_rows<VT, XT>(warp0, nrows, nw, row_ptr, col, val, X, ldx_, gc, [&](int64_t r, AT acc) {
+            if (lane == 0) store(r, acc);
+        });
+        return;
+    }
     const int64_t rstep = ROWSLOT ? nw * SLOTS : nw;
     for (int64_t rb = ROWSLOT ? warp0 * SLOTS : warp0; rb < nrows; rb += rstep) {
         const int64_t r = ROWSLOT ? rb + slot : rb;
@@ -69,30 +94,27 @@ __global__ void __launch_bounds__(256) k_spmm(int64_t nrows, const int64_t* __re
             row_times_x_tiles<KW, 1, VT, XT>(s, e, col, val, X, ldx_, blockIdx.y * KW, k, accv);
             acc = accv[0];
         }
-        if (mine && colok) {
-            double yr = alpha.x * (double)acc.x - alpha.y * (double)acc.y;
-            double yi = alpha.x * (double)acc.y + alpha.y * (double)acc.x;
-            if (has_sigma) {
-                XT xv = X[r * ldx_ + gc];
-                yr += sigma.x * (double)xv.x - sigma.y * (double)xv.y;
-                yi += sigma.x * (double)xv.y + sigma.y * (double)xv.x;
-            }
-            XT* yp = Y + r * ldy + (int64_t)gc * ycs;
-            if (has_beta) {
-                XT yv = *yp;
-                yr += beta.x * (double)yv.x - beta.y * (double)yv.y;
-                yi += beta.x * (double)yv.y + beta.y * (double)yv.x;
-            }
-            XT out;
-            out.x = yr;
-            out.y = yi;
-            *yp = out;
-        }
+        if (mine && colok) store(r, acc);
     }
 }
 
 // rows of at most this many entries on average run one row per slot
 constexpr int64_t SHORT_ROW = 16;
+
+// resident blocks per SM of a kernel (cached per device): a grid-stride launch then runs as
+// one wave with no tail of late blocks
+template <class K>
+static int resident_blocks(K kern, int threads) {
+    static int cache[EDX_MAX_DEVICES] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= EDX_MAX_DEVICES) return 4;
+    if (cache[dev] == 0) {
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, 0) != cudaSuccess || nb < 1) nb = 4;
+        cache[dev] = nb;
+    }
+    return cache[dev];
+}
 
 template <int KW, class VT, class XT>
 static int launch_spmm_t(const edx_csr* A, int k, const void* x, int64_t ldx_, void* y, int64_t ldy,
@@ -101,7 +123,9 @@ static int launch_spmm_t(const edx_csr* A, int k, const void* x, int64_t ldx_, v
     const bool rowslot = KW < 32 && A->nnz <= SHORT_ROW * A->nrows;
     const int64_t rows_per_warp = rowslot ? 32 / KW : 1;
     int64_t need = ((A->nrows + rows_per_warp - 1) / rows_per_warp * 32 + threads - 1) / threads;
-    int64_t maxb = (int64_t)num_sms() * 8;
+    const int res = rowslot ? resident_blocks(k_spmm<KW, VT, XT, true>, threads)
+                            : resident_blocks(k_spmm<KW, VT, XT, false>, threads);
+    int64_t maxb = (int64_t)num_sms() * res;
     int64_t bx = need < maxb ? need : maxb;
     if (bx < 1) bx = 1;
     dim3 grid((unsigned)bx, (unsigned)((k + KW - 1) / KW));

@@ -180,6 +180,67 @@ __device__ __forceinline__ void row_times_x_tiles(int64_t start, int64_t end, co
     }
 }
 
+// One column, long rows: a warp walks rows r0, r0 + rstep, ...; each row's first 128 entries
+// are held four per lane, and the next row's entries load while this row's x values are
+// gathered, so a row pays one memory latency instead of two.  Rows longer than 128
+// entries finish their tail with plain 32-entry rounds.  epi(r, sum) is called with the
+// row's sum in every lane.  Per lane the sum runs over entries lane, lane + 32, ... in order,
+// then the warp adds lanes by a butterfly, as row_times_x_tiles<1>.
+template <class VT, class XT, class Epi>
+__device__ __forceinline__ void spmv_rows(int64_t r0, int64_t r1, int64_t rstep, const int64_t* __restrict__ row_ptr,
+                                          const int32_t* __restrict__ col, const VT* __restrict__ val,
+                                          const XT* __restrict__ X, int64_t ldx_, int col0, Epi epi) {
+    using AT = typename Acc<VT, XT>::T;
+    const int lane = threadIdx.x & 31;
+    if (r0 >= r1) return;
+    int cc[4];
+    AT vv[4];
+    int64_t s = __ldg(row_ptr + r0), e = __ldg(row_ptr + r0 + 1);
+    auto load4 = [&](int64_t st, int64_t en, int* c4, AT* v4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t j = st + u * 32 + lane;
+            c4[u] = j < en ? ld_stream(col + j) : 0;
+            v4[u] = j < en ? to_acc(ld_stream(val + j), AT()) : zero_c<AT>();
+        }
+    };
+    load4(s, e, cc, vv);
+    for (int64_t r = r0; r < r1; r += rstep) {
+        const int64_t rn = r + rstep;
+        int64_t sn = 0, en = 0;
+        int cn[4];
+        AT vn[4];
+        if (rn < r1) {
+            sn = __ldg(row_ptr + rn);
+            en = __ldg(row_ptr + rn + 1);
+        }
+        load4(sn, en, cn, vn);  // next row's entries (none past the last row)
+        AT acc = zero_c<AT>();
+        AT xs[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            xs[u] = (s + u * 32 + lane < e) ? to_acc(ldx(X + (int64_t)cc[u] * ldx_ + col0), AT()) : zero_c<AT>();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc = fma_c(vv[u], xs[u], acc);
+        for (int64_t base = s + 128; base < e; base += 32) {  // tail of a long row
+            const int64_t j = base + lane;
+            if (j < e)
+                acc = fma_c(to_acc(ld_stream(val + j), AT()),
+                            to_acc(ldx(X + (int64_t)ld_stream(col + j) * ldx_ + col0), AT()), acc);
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) acc = xor_sum(acc, off);
+        epi(r, acc);
+        s = sn;
+        e = en;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            cc[u] = cn[u];
+            vv[u] = vn[u];
+        }
+    }
+}
+
 // Streaming loads of packed entry words (read once per product).
 __device__ __forceinline__ uint4 ld_stream4(const uint32_t* p) {
     uint4 v;

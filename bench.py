@@ -46,6 +46,13 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-packed", action="store_true", help="no packed forms of H_n, H_f (CSR products only)")
     ap.add_argument("--tiles", action="store_true", help="also offer the tiled layout of H_f to the autotuner")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving mix instead of the batched-RIXS step: Poisson arrivals of ED/XAS/RIXS jobs")
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-rate", type=float, default=50.0, help="offered arrivals per second")
+    ap.add_argument("--serve-seed", type=int, default=7)
+    ap.add_argument("--serve-workers", type=int, default=3)
+    ap.add_argument("--hbm-budget", type=float, default=150e9)
     ap.add_argument("--kernel-case", choices=["apply", "hf-shapes", "all"], default=None,
                     help="run only a small profiling case of the dominant kernels (for ncu)")
     return ap.parse_args()
@@ -580,6 +587,95 @@ def run_ours(args):
     dist.finalize()
 
 
+def serve_mix(args):
+    """The serving mix: seeded Poisson arrivals (rate --serve-rate) of ED, XAS and RIXS jobs on
+    impurity models of 16 to 22 valence spin-orbitals (10 d + 6..12 bath), N = norb/2 - 1 ..
+    norb/2 + 1, so Hilbert spaces of 1e4 to 4e6 states; 20 % of the jobs are RIXS or XAS on a
+    Hamiltonian an earlier job used, with new incident energies or polarisations."""
+    from edrixs_b200.serve import ModelSpec, Request
+    rng = np.random.default_rng(args.serve_seed)
+    jobs, used = [], []
+    t = 0.0
+    for _ in range(args.serve_requests):
+        t += rng.exponential(1.0 / args.serve_rate)
+        if used and rng.random() < 0.2:
+            spec = used[rng.integers(len(used))]
+            kind = "rixs" if rng.random() < 0.5 else "xas"
+        else:
+            kind = rng.choice(["ed", "xas", "rixs"], p=[0.4, 0.3, 0.3])
+            nbath = int(rng.choice([6, 8, 10] if kind == "rixs" else [6, 8, 10, 12]))
+            norb = 10 + nbath
+            spec = ModelSpec(nbath, norb // 2 + int(rng.integers(-1, 2)), int(rng.integers(1, 10 ** 6)))
+            used.append(spec)
+        ngs = int(rng.integers(1, 4))
+        if kind == "ed":
+            req = Request("ed", spec, ngs=4)
+        elif kind == "xas":
+            req = Request("xas", spec, ngs=ngs, eloss=np.linspace(-5.0, 15.0, 1000), gamma_c=0.3,
+                          pols=(int(rng.integers(0, 2)),), nkryl=200)
+        else:
+            pols = tuple(sorted(rng.choice(4, size=int(rng.integers(1, 5)), replace=False).tolist()))
+            req = Request("rixs", spec, ngs=ngs, omegas=np.sort(rng.uniform(0.0, 8.0, 8)),
+                          eloss=np.linspace(-0.5, 12.0, 1000), gamma_c=0.6, gamma_f=0.1, pols=pols, nkryl=150)
+        jobs.append((t, req))
+    return jobs
+
+
+def run_serve(args):
+    """Serving benchmark (one GPU): submit the mix at its arrival times to a running Server and
+    report completed requests per second over the makespan, with p50/p99 latency (queueing +
+    service) overall and per job kind."""
+    import math
+    from edrixs_b200.serve import Server
+    jobs = serve_mix(args)
+    srv = Server(hbm_budget=args.hbm_budget, workers=args.serve_workers).start()
+    futs = []
+    try:
+        t0 = time.perf_counter()
+        for ta, req in jobs:
+            dt = ta - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            futs.append(srv.submit(req))
+        failed = 0
+        errors = {}
+        for (_, req), f in zip(jobs, futs):
+            try:
+                f.result(timeout=1800)
+            except Exception as e:
+                failed += 1
+                key = f"{req.kind}: {type(e).__name__}: {str(e)[:160]}"
+                errors[key] = errors.get(key, 0) + 1
+        makespan = time.perf_counter() - t0
+    finally:
+        srv.shutdown()
+    recs = srv.records
+    lat = np.array([r["latency_s"] for r in recs]) * 1e3
+
+    def pct(a, q):
+        return round(float(np.percentile(a, q)), 1) if len(a) else None
+
+    by_kind = {}
+    for kind in ("ed", "xas", "rixs"):
+        rk = [r for r in recs if r["kind"] == kind]
+        lk = np.array([r["latency_s"] for r in rk]) * 1e3
+        sk = np.array([r["service_s"] for r in rk]) * 1e3
+        by_kind[kind] = {"n": len(rk), "p50_ms": pct(lk, 50), "p99_ms": pct(lk, 99), "service_p50_ms": pct(sk, 50)}
+    dims = [math.comb(10 + r.model.nbath, r.model.nelec) for _, r in jobs]
+    line = {"metric": "serving mix: completed requests/s & p50/p99 latency (queueing + service)",
+            "value": round(len(recs) / makespan, 3), "unit": "req/s", "higher_is_better": True, "n_gpus": 1,
+            "n_requests": len(jobs), "completed": len(recs), "failed": failed, "errors": errors,
+            "offered_rate": args.serve_rate, "makespan_s": round(makespan, 2),
+            "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)}, "by_kind": by_kind,
+            "coalesced_requests": int(sum(1 for r in recs if r["coalesced"] > 1)),
+            "dtype": "c128", "data": "synthetic (seeded SIAM inputs; reference atomic tensors)",
+            "config": {"workload": "ED/XAS/RIXS serving mix, norb 16-22, N = norb/2 +- 1, "
+                                   f"dim_i {min(dims)}..{max(dims)}, 20 % reuse of a resident Hamiltonian",
+                       "hbm_budget_gb": args.hbm_budget / 1e9, "workers": args.serve_workers,
+                       "seed": args.serve_seed}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -615,7 +711,9 @@ def run_reference(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.kernel_case == "hf-shapes":
+    if a.serve:
+        run_serve(a)
+    elif a.kernel_case == "hf-shapes":
         kernel_case_hf_shapes(a)
     elif a.kernel_case == "all":
         kernel_case_all(a)

@@ -336,7 +336,12 @@ def spmm(A: CSR, X, Y=None, alpha=1.0, sigma=0.0, beta=0.0, c64=False, col_group
         beta = 0.0
     Ym = Y.reshape(Y.shape[0], -1)
     vec_type = C64 if X.dtype == torch.complex64 else C128
-    assert Xm.stride(1) == 1 and Ym.stride(1) == 1
+    # rows must be contiguous; a single column's stride is irrelevant (torch leaves a (n, 1)
+    # slice of a column-major block with column stride n, and calls it contiguous)
+    if k > 1 and Xm.stride(1) != 1:
+        Xm = Xm.contiguous()
+    if k > 1 and Ym.stride(1) != 1:
+        raise ValueError("spmm: Y must be row-major (n, k)")
     al, sg, be = complex(alpha), complex(sigma), complex(beta)
     call("edx_spmm", ctypes.byref(A.desc(c64)), k, vec_type, _ptr(Xm), Xm.stride(0), _ptr(Ym), Ym.stride(0),
          al.real, al.imag, sg.real, sg.imag, be.real, be.imag, col_group, _stream())

@@ -81,12 +81,13 @@ class Resident:
         self.gs_v = None
         self.edge = None
         self.ops = {}
+        self.packed = {}             # "hi" / "hn" -> device.PackedMatrix (None: too many values)
         self.busy = 0
         self.last_used = time.monotonic()
 
     def nbytes(self):
         b = 0
-        for M in [self.Hi, self.Hn] + list(self.ops.values()):
+        for M in [self.Hi, self.Hn] + list(self.ops.values()) + list(self.packed.values()):
             if M is not None:
                 b += M.nbytes()
         if self.gs_v is not None:
@@ -105,6 +106,7 @@ class Resident:
                 self.bi = device.fock_unrank(s.nv, s.nelec)
                 self.Hi = device.build_csr(device.HAM_I, self.bi, self.terms["hop_i"], self.terms["coul_i"],
                                            num_val_orbs=s.nv)
+                self.packed["hi"] = device.pack(self.Hi)
             if self.gs_v is None or self.gs_v.shape[1] < ngs:
                 e, v = solvers.lowest_eigs(self.Hi, ngs, ngs, tol=1e-9)
                 self.gs_e, self.gs_v = np.asarray(e), v.contiguous()
@@ -112,6 +114,7 @@ class Resident:
                 self.bn = device.fock_unrank(s.nv, s.nelec + 1)
                 self.Hn = device.build_csr(device.HAM_N, self.bn, self.terms["hop_n"], self.terms["coul_n"],
                                            num_val_orbs=s.nv, num_core_orbs=6)
+                self.packed["hn"] = device.pack(self.Hn)
                 e_n, _ = solvers.lowest_eigs(self.Hn, 1, 1, tol=1e-6)
                 self.edge = float(e_n[0] - self.gs_e[0])
             # the resident is shared with other workers' streams: finish building it here
@@ -179,6 +182,7 @@ class Server:
     # -- public ---------------------------------------------------------------------------
     def start(self):
         device.require_cuda()
+        _warm_torch()
         self.sched = threading.Thread(target=self._schedule, daemon=True)
         self.sched.start()
         for i in range(self.workers):
@@ -310,7 +314,9 @@ class Server:
         pouts = sorted(set(siam_pol_out(p) for p in req.pols))
         P = rixs.RixsProblem(Hn=res.Hn, Hf=res.Hi, Din=[res.op("in", p) for p in pins],
                              Dout=[res.op("out", p) for p in pouts], gs_e=res.gs_e[:req.ngs],
-                             gs_v=res.gs_v[:, :req.ngs].contiguous())
+                             gs_v=res.gs_v[:, :req.ngs].contiguous(),
+                             packed={k: v for k, v in (("hf", res.packed.get("hi")), ("hn", res.packed.get("hn")))
+                                     if v is not None})
         out = rixs.rixs_spectra(P, allw, req.gamma_c, req.eloss, req.gamma_f, nkryl=req.nkryl,
                                 linsys_tol=req.linsys_tol, linsys_max=req.linsys_max, temperature=req.temperature)
         results = []
@@ -324,12 +330,27 @@ class Server:
     def _xas(self, r: Request, res: Resident):
         D = res.op("xas", r.pols[0])
         phi = device.spmm(D, res.gs_v[:, :r.ngs].contiguous())
-        kr = device.krylov(res.Hn, phi, r.nkryl)
+        pk = res.packed.get("hn")
+        kr = device.krylov(res.Hn, phi, r.nkryl, apply=dict(packed=pk) if pk is not None else None)
         w = rixs.boltz(res.gs_e[:r.ngs], r.temperature)
         grid = np.asarray(r.eloss, dtype=np.float64) + res.edge
         spec = device.cf_spectrum(kr.neff, kr.alpha, kr.beta, res.gs_e[:r.ngs], kr.norm.cpu().numpy(), w, grid,
                                   np.full(len(grid), r.gamma_c))
         return {"grid": grid, "spectrum": spec.cpu().numpy()}
+
+
+def _warm_torch():
+    """Run once, on the calling thread, every torch routine the solves use: torch loads some
+    of its linear-algebra backends lazily, and that first load must not happen in several
+    worker threads at once."""
+    A = torch.randn((8, 8), dtype=torch.complex128, device="cuda")
+    H = A + A.conj().T
+    torch.linalg.qr(A, mode="reduced")
+    torch.linalg.eigh(H)
+    torch.linalg.vector_norm(A, dim=0, keepdim=True)
+    torch.matmul(A, A)
+    torch.einsum("ij,j->i", A, A[0])
+    torch.cuda.synchronize()
 
 
 def siam_pol_in(p):

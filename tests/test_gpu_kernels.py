@@ -160,6 +160,22 @@ def test_spmm_short_rows(cuda, k):
     assert np.abs(Yt.cpu().numpy() - want).max() <= 1e-13 * np.abs(want).max()
 
 
+@pytest.mark.parametrize("k", [1, 2])
+def test_spmm_column_major_slices(hn_pair, k):
+    """X given as a column slice of a column-major block (what an eigensolver returns): one
+    column is used as is, wider slices are copied to row-major."""
+    import torch
+    from edrixs_b200 import device
+    ref, gpu = hn_pair
+    rng = np.random.default_rng(3)
+    B = rng.normal(size=(ref.nrows, 4)) + 1j * rng.normal(size=(ref.nrows, 4))
+    Bt = torch.from_numpy(B).cuda().T.contiguous().T
+    assert Bt.stride() == (1, ref.nrows)
+    Y = device.spmm(gpu, Bt[:, :k].contiguous())
+    want = np.stack([orc.matvec(ref, B[:, c]) for c in range(k)], axis=1)
+    assert np.abs(Y.cpu().numpy() - want).max() <= 1e-13 * np.abs(want).max()
+
+
 @pytest.mark.parametrize("k", [1, 8])
 def test_spmm_c64(hn_pair, k):
     import torch

@@ -91,6 +91,9 @@ _SIGS = {
     "edx_pack_count": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_int), vp, ctypes.c_size_t, vp]),
     "edx_pack_fill": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(Packed), vp, ctypes.c_size_t, vp]),
+    "edx_gs_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "edx_gs_dot": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp, ctypes.c_size_t, vp]),
+    "edx_gs_update": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp]),
     "edx_krylov_workspace": (ctypes.c_int, [i64, ctypes.c_int, ctypes.POINTER(KrylovOpts), ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_size_t)]),
     "edx_krylov": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.c_int, vp, ctypes.c_int, vp, vp, vp, vp,

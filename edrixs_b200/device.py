@@ -448,6 +448,27 @@ def minres(A: CSR, b, tol, maxit, alpha=1.0, sigma=0.0, c64=False):
     return x, it.value, res.value
 
 
+def gs_dot(V, m, W):
+    """C = V[:m]^H W for V (>= m, n) row-major basis vectors and W (n, k) row-major, k <= 8."""
+    n, k = W.shape
+    assert V.stride(1) == 1 and W.is_contiguous() and V.shape[1] == n
+    C = torch.empty((m, k), dtype=torch.complex128, device=W.device)
+    ws = ctypes.c_size_t(0)
+    call("edx_gs_workspace", m, k, ctypes.byref(ws))
+    w = _work(ws.value)
+    call("edx_gs_dot", _ptr(V), m, n, V.stride(0), _ptr(W), k, _ptr(C), _ptr(w), ws.value, _stream())
+    return C
+
+
+def gs_update(V, m, W, C):
+    """W -= V[:m]^T C in place."""
+    n, k = W.shape
+    assert V.stride(1) == 1 and W.is_contiguous() and V.shape[1] == n
+    Cc = C.contiguous()
+    call("edx_gs_update", _ptr(V), m, n, V.stride(0), _ptr(W), k, _ptr(Cc), _stream())
+    return W
+
+
 def cf_spectrum(neff, alpha, beta, e0, norm, weight, omega, gamma, per_set=False):
     """Continued fraction of get_spectra_from_poles on the device.
     alpha/beta: (nset, ld) float64; returns (ngrid,) or (nset, ngrid)."""

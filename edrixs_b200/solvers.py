@@ -6,7 +6,9 @@ thick-restart Lanczos:
 
 * the Krylov block is expanded by one SpMM of width b per step (libedx ``edx_spmm``);
 * every new block is orthogonalised against the whole basis twice (classical Gram-Schmidt,
-  CGS2) -- a dense tall-skinny contraction done with cuBLAS ZGEMM on the FP64 tensor cores;
+  CGS2): tall-skinny contractions C = V^H W and W -= V^T C that libedx runs as single
+  bandwidth-bound passes over the basis (``edx_gs_dot`` / ``edx_gs_update``), then the
+  block is factorised by CholeskyQR2;
 * the projected matrix T = V^H H V is accumulated from those coefficients, so after a
   restart the kept Ritz vectors and their coupling to the residual block are exact;
 * Ritz pairs are accepted when || H u - theta u || <= tol; the block size b >= the
@@ -24,6 +26,31 @@ from . import device
 def _qr(W):
     Q, R = torch.linalg.qr(W, mode="reduced")
     return Q, R
+
+
+def _cholqr2(W):
+    """W = Q R for a tall-skinny block by CholeskyQR2 (Fukaya, Nakatsukasa, Yanagisawa,
+    Yamamoto 2014): twice, R from the Cholesky factor of the small Gram matrix W^H W and
+    Q = W R^-1.  Two passes over W instead of a Householder factorisation, which is slow for
+    millions of rows and a few columns.  A block too ill-conditioned for it (a Krylov space
+    about to break down) goes to Householder QR."""
+    k = W.shape[1]
+    Q = W
+    Rt = np.eye(k, dtype=np.complex128)
+    for _ in range(2):
+        G = (Q.conj().T @ Q).cpu().numpy()
+        G = 0.5 * (G + G.conj().T)
+        try:
+            L = np.linalg.cholesky(G)
+        except np.linalg.LinAlgError:
+            return _qr(W)
+        R = L.conj().T
+        d = np.abs(np.diag(R))
+        if not np.all(np.isfinite(d)) or d.min() <= 1e-7 * d.max():
+            return _qr(W)
+        Q = Q @ torch.from_numpy(np.linalg.inv(R)).to(W.device)
+        Rt = R @ Rt
+    return Q.contiguous(), torch.from_numpy(Rt).to(W.device)
 
 
 def dense_eigs(H: device.CSR, nev):
@@ -63,14 +90,14 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
     for restart in range(max_restarts):
         while j + b <= mmax:
             X = V[j:j + b].T.contiguous()
-            W = device.spmm(H, X, c64=c64)
-            Vb = V[:j + b]
-            C = Vb.conj() @ W
-            W = W - Vb.T @ C
-            C2 = Vb.conj() @ W
-            W = W - Vb.T @ C2
+            W = device.spmm(H, X, c64=c64).contiguous()
+            # classical Gram-Schmidt twice against the whole basis (libedx: one pass over V each)
+            C = device.gs_dot(V, j + b, W)
+            device.gs_update(V, j + b, W, C)
+            C2 = device.gs_dot(V, j + b, W)
+            device.gs_update(V, j + b, W, C2)
             C = C + C2
-            Q, R = _qr(W)
+            Q, R = _cholqr2(W)
             V[j + b:j + 2 * b] = Q.T
             T[:j + b, j:j + b] = C.cpu().numpy()
             T[j + b:j + 2 * b, j:j + b] = R.cpu().numpy()

@@ -213,6 +213,22 @@ int edx_pack_count(const edx_csr* A, int64_t* nnz_off, int* nval, int* vbits, vo
 int edx_pack_fill(const edx_csr* A, edx_packed* P, void* d_work, size_t work_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------- */
+/* Block Gram-Schmidt for the ground-state eigensolver (the reorthogonalisation inside      */
+/* ARPACK's pznaupd, src/arpack.f90:76, done here for the thick-restart Lanczos)          */
+/* ---------------------------------------------------------------------------------- */
+
+/* V: m basis vectors of length n, vector i at d_V[i*ldv .. i*ldv + n) (complex128).
+ * W: n x k block, row-major (d_W[r*k + c]), 1 <= k <= 8.  C: m x k row-major.
+ * edx_gs_dot:    C = V^H W   (deterministic: fixed row chunks per block, fixed final tree)
+ * edx_gs_update: W -= V^T C
+ * (m + 512) * k * 16 bytes must fit in 200 KB. */
+int edx_gs_workspace(int m, int k, size_t* bytes);
+int edx_gs_dot(const double* d_V, int m, int64_t n, int64_t ldv, const double* d_W, int k, double* d_C,
+               void* d_work, size_t work_bytes, void* stream);
+int edx_gs_update(const double* d_V, int m, int64_t n, int64_t ldv, double* d_W, int k, const double* d_C,
+                  void* stream);
+
+/* ---------------------------------------------------------------------------------- */
 /* Lanczos / Krylov                                                                     */
 /* ---------------------------------------------------------------------------------- */
 

@@ -58,6 +58,14 @@ def parse():
     ap.add_argument("--serve-seed", type=int, default=7)
     ap.add_argument("--serve-workers", type=int, default=3)
     ap.add_argument("--hbm-budget", type=float, default=150e9)
+    ap.add_argument("--scale", action="store_true",
+                    help="XAS and RIXS at scale: 10 + 16 orbitals, N = 13 (10.4 M ground, 57.9 M intermediate "
+                         "states); complex64 CSR vs FP64 CSR vs the packed FP64 form")
+    ap.add_argument("--scale-nbath", type=int, default=16)
+    ap.add_argument("--scale-nelec", type=int, default=13)
+    ap.add_argument("--scale-omega", type=int, default=32)
+    ap.add_argument("--scale-c64-omega", type=int, default=8,
+                    help="incident energies (a subset of --scale-omega) of the complex64 RIXS comparison")
     ap.add_argument("--kernel-case", choices=["apply", "hf-shapes", "all"], default=None,
                     help="run only a small profiling case of the dominant kernels (for ncu)")
     return ap.parse_args()
@@ -196,17 +204,19 @@ def setup_gpu(args, ngs=3):
                           want_c64=args.c64)
     Din = [device.build_csr(device.TRANS_I, bn, d, right=bi, num_val_orbs=nv, num_core_orbs=6) for d in t["din"]]
     Dout = [device.build_csr(device.TRANS_F, bi, d, right=bn, num_val_orbs=nv, num_core_orbs=6) for d in t["dout"]]
-    gs_e, gs_v = solvers.lowest_eigs(Hf, ngs, ngs, tol=1e-9)
-    e_n, _ = solvers.lowest_eigs(Hn, 1, 1, tol=1e-6)
-    edge = float(e_n[0] - gs_e[0])
-    P = rixs.RixsProblem(Hn=Hn, Hf=Hf, Din=Din, Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v.contiguous())
-    if args.tiles and not args.c64:
-        P.tiles["hf"] = device.tiles_for(Hf, bi)
+    packed = {}
     if not args.no_packed and not args.c64:
         for name, M in (("hf", Hf), ("hn", Hn)):
             pm = device.pack(M)
             if pm is not None:
-                P.packed[name] = pm
+                packed[name] = pm
+    gs_e, gs_v = solvers.lowest_eigs(Hf, ngs, ngs, tol=1e-9, packed=packed.get("hf"))
+    e_n, _ = solvers.lowest_eigs(Hn, 1, 1, tol=1e-6, packed=packed.get("hn"))
+    edge = float(e_n[0] - gs_e[0])
+    P = rixs.RixsProblem(Hn=Hn, Hf=Hf, Din=Din, Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v.contiguous())
+    P.packed.update(packed)
+    if args.tiles and not args.c64:
+        P.tiles["hf"] = device.tiles_for(Hf, bi)
     omegas = edge - 2.0 + np.linspace(0.0, 10.0, args.n_omega)
     eloss = np.linspace(-0.5, 12.0, args.n_eloss)
     torch.cuda.synchronize()
@@ -331,7 +341,10 @@ def spmv_roofline_of(A, peak, label):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
-    byts = A.nnz * 20 + (A.nrows + 1) * 8 + 2 * A.nrows * 16
+    if isinstance(A, device.PackedMatrix):  # entries, row pointers, value table, diagonal, x, y
+        byts = A.nnz * (6 if A.wide else 4) + (A.nrows + 1) * 8 + A.vals.numel() * 16 + 3 * A.nrows * 16
+    else:
+        byts = A.nnz * 20 + (A.nrows + 1) * 8 + 2 * A.nrows * 16
     ach = byts / (ms / 1e3) / 1e9
     return dict(kernel=label, bound="hbm", achieved=round(ach, 1),
                 peak=peak, unit="GB/s", frac=round(ach / peak, 4), bytes_per_launch=int(byts),
@@ -619,9 +632,30 @@ def run_ed(args):
     torch.cuda.synchronize()
     t_fock, t_build, t_pack = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3])
     roof = spmv_roofline_of(H, peak, f"k_spmm<1> on H (one column, complex128 CSR, dim {H.nrows})")
+    roof_p = None
+    if Pk is not None:
+        form = "wide" if Pk.wide else "narrow"
+        roof_p = spmv_roofline_of(Pk, peak, f"k_spmm_packed<1> on H (one column, {form} packed form, dim {H.nrows})")
+    # the eigensolver's block product (k = nev columns) on both forms
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    X = torch.randn((H.nrows, args.ed_nev), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    blk_us = {}
+    for name, A in (("csr", H), ("packed", Pk)):
+        if A is None:
+            continue
+        for _ in range(3):
+            device.spmm(A, X)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            device.spmm(A, X)
+        e1.record()
+        torch.cuda.synchronize()
+        blk_us[name] = round(e0.elapsed_time(e1) / 10 * 1e3, 1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e, v = solvers.lowest_eigs(H, args.ed_nev, args.ed_nev, tol=1e-10)
+    e, v = solvers.lowest_eigs(H, args.ed_nev, args.ed_nev, tol=1e-10, packed=Pk)
     torch.cuda.synchronize()
     t_eig = time.perf_counter() - t0
     Hv = device.spmm(H, v.contiguous())
@@ -636,7 +670,9 @@ def run_ed(args):
             "nnz": H.nnz, "csr_gb": round(H.nbytes() / 1e9, 3),
             "packed_gb": round(Pk.nbytes() / 1e9, 3) if Pk is not None else None,
             "setup_ms": {"fock_unrank": round(t_fock, 2), "csr_build": round(t_build, 2), "pack": round(t_pack, 2)},
-            "spmv_roofline": dict(roof, peak_source=peak_kind)}
+            "spmv_roofline": dict(roof, peak_source=peak_kind),
+            "spmv_packed_roofline": dict(roof_p, peak_source=peak_kind) if roof_p else None,
+            "eig_products": "packed" if Pk is not None else "csr", "block_spmm_us": blk_us}
     print(json.dumps(line), flush=True)
 
 
@@ -672,6 +708,166 @@ def serve_mix(args):
                           eloss=np.linspace(-0.5, 12.0, 1000), gamma_c=0.6, gamma_f=0.1, pols=pols, nkryl=150)
         jobs.append((t, req))
     return jobs
+
+
+def run_scale(args):
+    """Mixed precision at scale.  10 impurity + 16 bath spin-orbitals, N = 13: the ground
+    sector holds C(26, 13) = 10,400,600 states (948 M nonzeros) and the intermediate sector
+    (N_v = 14, one 2p hole) 6 x C(26, 14) = 57,946,200 states with about 5.7 G nonzeros:
+    114 GB as a complex128 CSR, 68 GB as complex64 + int32 columns, 36 GB in the wide packed
+    form (exact FP64 values).  Steps, each timed with the device synchronised:
+      1. Fock bases, H_i build and packing, the 3 lowest eigenpairs (packed products);
+      2. D_in(pol_in)|g> seeds (6 columns), H_n as a complex128 CSR;
+      3. XAS: 200-step Lanczos of H_n on the seeds with FP64 CSR products (the reference's
+         arithmetic), then with complex64 products (the CSR converted in place);
+      4. RIXS with complex64 H_n products on a subset of the incident energies;
+      5. H_n rebuilt and packed (wide form), XAS on it, and the full 32-omega_in RIXS on the
+         packed forms (two-pass streaming of D_out^+ v_i: storing it for every v_i would
+         take terabytes).
+    Errors: XAS spectra (1000 points, Gamma = 0.3) of the complex64 and packed products
+    against the FP64 CSR products; RIXS spectra with complex64 H_n products against the
+    packed FP64 ones on the shared incident energies."""
+    import gc
+    import math
+    import torch
+    from edrixs_b200 import device, rixs, solvers
+    nb, N = args.scale_nbath, args.scale_nelec
+    m, t = workload_terms(nb, N)
+    nv = m.nv
+    res = {"config": {"workload": f"XAS + RIXS at scale: 10 impurity + {nb} bath spin-orbitals, N={N}",
+                      "dim_i": math.comb(nv, N), "dim_n": 6 * math.comb(nv, N + 1)}}
+    tm = {}
+
+    def tick():
+        torch.cuda.synchronize()
+        return time.perf_counter()
+
+    def free():
+        gc.collect()
+        torch.cuda.empty_cache()
+
+    def gb(x):
+        return round(x / 1e9, 2)
+
+    # 1. ground states on the packed H_i
+    t0 = tick()
+    bi = device.fock_unrank(nv, N)
+    Hi = device.build_csr(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
+    t1 = tick()
+    Pi = device.pack(Hi)
+    t2 = tick()
+    res["H_i"] = {"nnz": Hi.nnz, "csr_gb": gb(Hi.nbytes()), "packed_gb": gb(Pi.nbytes()),
+                  "packed_form": "wide" if Pi.wide else "narrow", "distinct_values": Pi.vals.numel()}
+    del Hi
+    free()
+    gs_e, gs_v = solvers.lowest_eigs(Pi, 3, 3, tol=1e-9)
+    t3 = tick()
+    tm.update(hi_build_s=t1 - t0, hi_pack_s=t2 - t1, ground_states_s=t3 - t2)
+    res["gs_e"] = [float(x) for x in gs_e]
+    # 2. seeds and H_n (complex128 CSR)
+    t0 = tick()
+    bn = device.fock_unrank(nv, N + 1)
+    seeds = []
+    for d in t["din"]:
+        D = device.build_csr(device.TRANS_I, bn, d, right=bi, num_val_orbs=nv, num_core_orbs=6)
+        seeds.append(device.spmm(D, gs_v))
+        del D
+    seeds = torch.cat(seeds, dim=1).contiguous()
+    free()
+    t1 = tick()
+    Hn = device.build_csr(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    t2 = tick()
+    tm.update(seeds_s=t1 - t0, hn_build_s=t2 - t1)
+    res["H_n"] = {"nnz": Hn.nnz, "csr_c128_gb": gb(Hn.nbytes()), "csr_c64_gb": gb(Hn.nbytes(c64=True))}
+    nk = 200
+
+    def xas(A, c64=False):
+        ta = tick()
+        kr = device.krylov(A, seeds, nk, c64=c64, timing=True)
+        return kr, tick() - ta
+
+    xa, tm["xas_fp64_csr_s"] = xas(Hn)
+    tm["xas_fp64_csr_apply_ms_per_step"] = xa.apply_ms / max(xa.apply_launches, 1)
+    # edge from the lowest Ritz value of the XAS recurrence of the ground state
+    ne = int(xa.neff[0].item())
+    a0, b0 = xa.alpha[0, :ne].cpu().numpy(), xa.beta[0, :ne - 1].cpu().numpy()
+    edge = float(np.linalg.eigvalsh(np.diag(a0) + np.diag(b0, 1) + np.diag(b0, -1))[0] - gs_e[0])
+    grid = edge - 2.0 + np.linspace(0.0, 10.0, 1000)
+    w = rixs.boltz(gs_e, 300.0)
+
+    def xas_spec(kr):  # per seed column; the XAS spectrum of pol p is the Boltzmann sum of its gs
+        sp = device.cf_spectrum(kr.neff, kr.alpha, kr.beta, np.tile(gs_e, 2), kr.norm.cpu().numpy(), np.tile(w, 2),
+                                grid, np.full(len(grid), 0.3), per_set=True).cpu().numpy()
+        return sp.reshape(2, 3, -1).sum(axis=1)
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+    sa = xas_spec(xa)
+    # 3b. complex64 products: H_n rebuilt with complex64 values only
+    del Hn
+    free()
+    t0 = tick()
+    Hn = device.build_csr(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6,
+                          values="c64")
+    tm["hn_build_c64_s"] = tick() - t0
+    xb, tm["xas_c64_csr_s"] = xas(Hn, c64=True)
+    tm["xas_c64_csr_apply_ms_per_step"] = xb.apply_ms / max(xb.apply_launches, 1)
+    sb = xas_spec(xb)
+    res["xas"] = {"steps": nk, "columns": seeds.shape[1], "grid_points": len(grid), "gamma": 0.3,
+                  "c64_vs_fp64_rel_linf": rel(sb, sa),
+                  "alpha_c64_vs_fp64_first10_max_rel": float(
+                      (torch.abs(xb.alpha[:, :10] - xa.alpha[:, :10]) / torch.abs(xa.alpha[:, :10])).max())}
+    # 4. RIXS, complex64 H_n products, on a subset of the incident energies
+    Dout = [device.build_csr(device.TRANS_F, bi, d, right=bn, num_val_orbs=nv, num_core_orbs=6) for d in t["dout"]]
+    omegas = edge - 2.0 + np.linspace(0.0, 10.0, args.scale_omega)
+    sub = np.linspace(0, args.scale_omega - 1, args.scale_c64_omega).round().astype(int)
+    eloss = np.linspace(-0.5, 12.0, 2000)
+    kw = dict(nkryl=150, linsys_tol=1e-10, linsys_max=1000, temperature=300.0, stream=True, timing=True)
+    P = rixs.RixsProblem(Hn=Hn, Hf=Pi, Din=[], Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v)
+    P.packed["hf"] = Pi
+    t0 = tick()
+    rb = rixs.rixs_spectra(P, omegas[sub], 0.6, eloss, 0.1, c64=True, c64_final=False, seeds=seeds,
+                           final_block=128, **kw)
+    tm["rixs_c64_s"] = tick() - t0
+    # 5. packed FP64: XAS and the full RIXS request.  Only the seeds stay resident while the
+    # complex128 CSR of H_n and its packed form coexist; H_i and D_out are rebuilt after.
+    del P, Hn, xa, xb, Dout, Pi
+    free()
+    t0 = tick()
+    Hn = device.build_csr(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    t1 = tick()
+    Pn = device.pack(Hn)
+    t2 = tick()
+    del Hn
+    free()
+    Hi = device.build_csr(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
+    Pi = device.pack(Hi)
+    del Hi
+    free()
+    Dout = [device.build_csr(device.TRANS_F, bi, d, right=bn, num_val_orbs=nv, num_core_orbs=6) for d in t["dout"]]
+    tm.update(hn_rebuild_s=t1 - t0, hn_pack_s=t2 - t1, hi_dout_rebuild_s=tick() - t2)
+    res["H_n"].update(packed_gb=gb(Pn.nbytes()), packed_form="wide" if Pn.wide else "narrow",
+                      distinct_values=Pn.vals.numel())
+    xc, tm["xas_packed_s"] = xas(Pn)
+    tm["xas_packed_apply_ms_per_step"] = xc.apply_ms / max(xc.apply_launches, 1)
+    res["xas"]["packed_vs_fp64_rel_linf"] = rel(xas_spec(xc), sa)
+    del xc
+    P = rixs.RixsProblem(Hn=Pn, Hf=Pi, Din=[], Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v)
+    P.packed.update(hn=Pn, hf=Pi)
+    t0 = tick()
+    rc = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, seeds=seeds, final_block=64, **kw)
+    tm["rixs_packed_s"] = tick() - t0
+    npts = len(omegas) * 12
+    res["rixs"] = {"omega_in": len(omegas), "points": npts, "minres_iters_max": int(rc.iters.max()),
+                   "hn_lanczos_steps": rc.krylov_steps, "streamed": rc.stats["streamed"],
+                   "points_per_s": round(npts / tm["rixs_packed_s"], 3),
+                   "c64_vs_packed_fp64_rel_linf": rel(rb.spectra, rc.spectra[sub]),
+                   "c64_subset_omega_in": len(sub),
+                   "hn_apply_ms_total": rc.stats.get("hn_apply_ms"), "hf_apply_ms_total": rc.stats.get("hf_apply_ms")}
+    res["times_s"] = {k: round(v, 3) for k, v in tm.items()}
+    res["peak_device_gb"] = gb(torch.cuda.max_memory_allocated())
+    print(json.dumps(res), flush=True)
 
 
 def run_serve(args):
@@ -766,6 +962,8 @@ if __name__ == "__main__":
     a = parse()
     if a.serve:
         run_serve(a)
+    elif a.scale:
+        run_scale(a)
     elif a.ed:
         run_ed(a)
     elif a.kernel_case == "hf-shapes":

@@ -50,7 +50,7 @@ class Tiles(ctypes.Structure):
 
 class Packed(ctypes.Structure):
     _fields_ = [("nrows", i64), ("nnz", i64), ("row_ptr", vp), ("ent", vp), ("vbits", ctypes.c_int),
-                ("nval", ctypes.c_int), ("vals", vp), ("diag", vp)]
+                ("nval", ctypes.c_int), ("vals", vp), ("diag", vp), ("vidx", vp)]
 
 
 class KrylovOpts(ctypes.Structure):
@@ -61,7 +61,9 @@ class KrylovOpts(ctypes.Structure):
                 ("apply_col_group", ctypes.c_int), ("apply_threads", ctypes.c_int),
                 ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int),
                 ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int),
-                ("apply_layout", ctypes.POINTER(Tiles)), ("apply_packed", ctypes.POINTER(Packed))]
+                ("apply_layout", ctypes.POINTER(Tiles)), ("apply_packed", ctypes.POINTER(Packed)),
+                ("proj_window", ctypes.c_int), ("nacc", ctypes.c_int), ("acc_col", vp), ("acc_coef", vp),
+                ("acc_out", ctypes.POINTER(vp)), ("acc_ld", i64)]
 
 
 _SIGS = {
@@ -88,9 +90,12 @@ _SIGS = {
                                        ctypes.POINTER(i64), ctypes.POINTER(i64), vp, ctypes.c_size_t, vp]),
     "edx_tiles_fill": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(Tiles), vp, ctypes.c_size_t, vp]),
     "edx_pack_workspace": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(ctypes.c_size_t)]),
-    "edx_pack_count": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_int),
-                                      ctypes.POINTER(ctypes.c_int), vp, ctypes.c_size_t, vp]),
+    "edx_pack_count": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.c_int, ctypes.POINTER(i64),
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp, ctypes.c_size_t,
+                                      vp]),
     "edx_pack_fill": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(Packed), vp, ctypes.c_size_t, vp]),
+    "edx_spmm_packed": (ctypes.c_int, [ctypes.POINTER(Packed), ctypes.c_int, vp, i64, vp, i64, dbl, dbl, dbl, dbl,
+                                       dbl, dbl, ctypes.c_int, vp]),
     "edx_gs_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "edx_gs_dot": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp, ctypes.c_size_t, vp]),
     "edx_gs_update": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp]),

@@ -35,15 +35,40 @@ def up_to_date():
 
 
 def build(force=False, verbose=False, extra=()):
+    """Compile every .cu to an object in parallel (one nvcc per source), then link."""
     if not force and up_to_date():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
     host_cc = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
-    cmd = [nvcc(), "-O3", "-std=c++17", "-lineinfo", "-shared", "-Xcompiler", "-fPIC",
-           "-ccbin", host_cc, *ARCH, "-I", os.path.join(ROOT, "include"), *extra,
-           "-cudart", "static", "-o", LIB + ".tmp", *sources()]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [nvcc(), "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", host_cc, *ARCH,
+             "-I", os.path.join(ROOT, "include"), *extra]
+    jobs = []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        jobs.append((src, obj, flags + ["-c", src, "-o", obj]))
+
+    def run(job):
+        src, obj, cmd = job
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, r
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(run, jobs))
+    for src, r in results:
+        if verbose or r.returncode != 0:
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, f"nvcc {os.path.basename(src)}")
+    link = [nvcc(), "-shared", "-ccbin", host_cc, *ARCH, "-cudart", "static", "-o", LIB + ".tmp",
+            *[obj for _, obj, _ in jobs]]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

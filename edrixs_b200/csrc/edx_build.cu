@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256) k_build(BuildK p, int32_t* __restrict__ r
                 }
                 const int64_t dst = row_ptr[r] + nu + __popc(m & lt);
                 col_out[dst] = (int32_t)c;
-                val_out[dst] = sum;
+                if (val_out) val_out[dst] = sum;
                 if (val32_out) val32_out[dst] = make_float2((float)sum.x, (float)sum.y);
             }
             nu += __popc(m);
@@ -584,7 +584,7 @@ extern "C" int edx_build_fill(const edx_build_desc* d, int cap, const int64_t* d
                               double* d_val, float* d_val64, void* d_work, size_t work_bytes, void* stream) {
     int rc = validate(d);
     if (rc) return rc;
-    EDX_REQUIRE(d_row_ptr && d_col && d_val, "edx_build_fill: NULL output");
+    EDX_REQUIRE(d_row_ptr && d_col && (d_val || d_val64), "edx_build_fill: NULL output");
     cudaStream_t st = as_stream(stream);
     BuildWs w;
     if ((rc = carve(d, d_work, work_bytes, w))) return rc;

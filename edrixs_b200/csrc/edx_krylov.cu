@@ -167,15 +167,7 @@ __global__ void __launch_bounds__(NT) k_lanczos_apply(int64_t n, const int64_t* 
 // Same row mapping and epilogue as k_lanczos_apply.  The distinct values are copied to shared
 // memory first; the diagonal term d_r v_r is added in the epilogue, where V_cur[r] is read
 // anyway for alpha.
-struct PackedView {
-    const int64_t* row_ptr;
-    const uint32_t* ent;
-    const double2* vals;
-    const double2* diag;
-    int vbits, nval;
-};
-
-template <int KW, int TG, int NT>
+template <int KW, int TG, int NT, bool WIDE>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_lanczos_apply_packed(int64_t n, PackedView M, const double2* __restrict__ Vc,
                                                              double2* __restrict__ Vp, KrylovState S, int it,
                                                              int chunked) {
@@ -211,7 +203,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_lanczos_apply_packed(int64_t 
     for (int64_t r = r0; r < r1; r += rstep) {
         const int64_t s = __ldg(M.row_ptr + r), e = __ldg(M.row_ptr + r + 1);
         double2 acc[TG];
-        row_times_x_packed<KW, TG>(s, e, M.ent, M.vbits, pk_tab, Vc, k, col0, k, acc);
+        row_times_x_packed<KW, TG, WIDE>(s, e, M.ent, M.vidx, M.vbits, pk_tab, Vc, k, col0, k, acc);
         if (lane < KW) {
             const double2 d = __ldg(M.diag + r);
 #pragma unroll
@@ -531,6 +523,25 @@ __global__ void k_proj_scale(int64_t m, int k, int64_t maxn, int i, double2* __r
     }
 }
 
+// streaming projections: out[r * ld + s] += sum_{b < nb} coef[s * maxn + i0 + b] *
+// win[(c * B + b) * m + r], c = acc_col[s]; win holds the last nb projected vectors
+__global__ void k_proj_accum(int64_t m, int B, int nb, int i0, int64_t maxn, int nacc,
+                             const int32_t* __restrict__ acc_col, const double2* __restrict__ coef,
+                             const double2* __restrict__ win, double2* __restrict__ out, int64_t ld) {
+    const int64_t total = m * nacc;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / nacc;
+        const int s = (int)(e - r * nacc);
+        const double2* w = win + (int64_t)acc_col[s] * B * m + r;
+        const double2* cf = coef + (int64_t)s * maxn + i0;
+        double2* o = out + r * ld + s;
+        double2 a = *o;
+        for (int b = 0; b < nb; ++b) a = fma_c(cf[b], w[(int64_t)b * m], a);
+        *o = a;
+    }
+}
+
 // ---- start vectors: norm and normalisation --------------------------------------------
 template <int KW>
 __global__ void __launch_bounds__(KT) k_colnorm(int64_t n, const double2* __restrict__ V0, KrylovState S) {
@@ -718,10 +729,10 @@ static int apply_v(const edx_csr* A, const double2* Vc, double2* Vp, const Krylo
     return fail(EDX_ERR_INVALID, "krylov: bad column group %d", cfg.kw);
 }
 
-template <int KW, int TG, int NT>
+template <int KW, int TG, int NT, bool WIDE>
 static int launch_packed_nt(int64_t n, const PackedView& M, const double2* Vc, double2* Vp, const KrylovState& S,
                             int it, const ApplyCfg& cfg, cudaStream_t st) {
-    auto kern = k_lanczos_apply_packed<KW, TG, NT>;
+    auto kern = k_lanczos_apply_packed<KW, TG, NT, WIDE>;
     static bool attr_set[EDX_MAX_DEVICES] = {};
     int dev = 0;
     EDX_CUDA(cudaGetDevice(&dev));
@@ -741,14 +752,18 @@ static int launch_packed_nt(int64_t n, const PackedView& M, const double2* Vc, d
 template <int KW, int TG>
 static int launch_packed(int64_t n, const PackedView& M, const double2* Vc, double2* Vp, const KrylovState& S,
                          int it, const ApplyCfg& cfg, cudaStream_t st) {
-    if (cfg.threads == 1024) return launch_packed_nt<KW, TG, 1024>(n, M, Vc, Vp, S, it, cfg, st);
-    return launch_packed_nt<KW, TG, 256>(n, M, Vc, Vp, S, it, cfg, st);
+    if (M.vbits == 0) {
+        if (cfg.threads == 1024) return launch_packed_nt<KW, TG, 1024, true>(n, M, Vc, Vp, S, it, cfg, st);
+        return launch_packed_nt<KW, TG, 256, true>(n, M, Vc, Vp, S, it, cfg, st);
+    }
+    if (cfg.threads == 1024) return launch_packed_nt<KW, TG, 1024, false>(n, M, Vc, Vp, S, it, cfg, st);
+    return launch_packed_nt<KW, TG, 256, false>(n, M, Vc, Vp, S, it, cfg, st);
 }
 
 static int apply_packed(const edx_packed* P, const double2* Vc, double2* Vp, const KrylovState& S, int it,
                         const ApplyCfg& cfg, cudaStream_t st) {
     const PackedView M{P->row_ptr, P->ent, reinterpret_cast<const double2*>(P->vals),
-                       reinterpret_cast<const double2*>(P->diag), P->vbits, P->nval};
+                       reinterpret_cast<const double2*>(P->diag), P->vbits, P->nval, P->vidx};
     const int64_t n = P->nrows;
     switch (cfg.kw) {
     case 1: return launch_packed<1, 1>(n, M, Vc, Vp, S, it, cfg, st);
@@ -892,6 +907,13 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
         if (rc) return rc;
         EDX_REQUIRE(opts->proj[p].ncols == A->nrows, "edx_krylov: projection %d has wrong width", p);
     }
+    const int win = (opts && nproj > 0 && opts->proj_window > 0) ? opts->proj_window : 0;
+    if (win) {
+        EDX_REQUIRE(opts->nacc >= 1 && opts->acc_col && opts->acc_coef && opts->acc_out && opts->acc_ld >= opts->nacc,
+                    "edx_krylov: streaming projections need nacc, acc_col, acc_coef, acc_out and acc_ld >= nacc");
+        for (int p = 0; p < nproj; ++p)
+            EDX_REQUIRE(opts->acc_out[p], "edx_krylov: accumulator %d missing", p);
+    }
     cudaStream_t st = as_stream(stream);
     const int64_t n = A->nrows;
     ApplyCfg cfg;
@@ -923,7 +945,8 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     if (packed) {
         EDX_REQUIRE(packed->nrows == n && packed->row_ptr && packed->diag &&
                         (packed->nnz == 0 || (packed->ent && packed->vals)) && packed->nval >= 0 &&
-                        packed->nval <= EDX_PACK_VALUES_MAX && packed->vbits >= 1 && packed->vbits <= 31,
+                        packed->nval <= EDX_PACK_VALUES_MAX && packed->vbits >= 0 && packed->vbits <= 31 &&
+                        (packed->vbits > 0 || packed->nnz == 0 || packed->vidx),
                     "edx_krylov: apply_packed does not describe this matrix");
     }
     const int kw = pow2_kw(k);  // layout of the element-wise recurrence kernels
@@ -971,21 +994,42 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
                                                            opts->shift_tol, opts->shift_maxit);
         EDX_CHECK_LAUNCH();
     }
+    // streaming projections: slots [0, win_n) of the window hold v_{win_i0 ..}
+    int win_i0 = 0, win_n = 0;
+    auto flush = [&]() -> int {
+        if (!win || win_n == 0) return EDX_OK;
+        for (int p = 0; p < nproj; ++p) {
+            const int64_t m = opts->proj[p].nrows;
+            const int64_t tot = m * (int64_t)opts->nacc;
+            const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)num_sms() * 16);
+            k_proj_accum<<<blocks, 256, 0, st>>>(m, win, win_n, win_i0, maxn, opts->nacc, opts->acc_col,
+                                                 reinterpret_cast<const double2*>(opts->acc_coef),
+                                                 reinterpret_cast<const double2*>(opts->proj_out[p]),
+                                                 reinterpret_cast<double2*>(opts->acc_out[p]), opts->acc_ld);
+            EDX_CHECK_LAUNCH();
+        }
+        win_i0 += win_n;
+        win_n = 0;
+        return EDX_OK;
+    };
     auto project = [&](const double2* V, int i) -> int {
+        const int slot = win ? i - win_i0 : i;
+        const int64_t depth = win ? win : maxn;
         for (int p = 0; p < nproj; ++p) {
             const edx_csr* P = &opts->proj[p];
-            double2* out = reinterpret_cast<double2*>(opts->proj_out[p]) + (int64_t)i * P->nrows;
-            int r2 = spmm_dispatch(P, k, EDX_C128, V, k, out, 1, (int64_t)maxn * P->nrows,
+            double2* out = reinterpret_cast<double2*>(opts->proj_out[p]) + (int64_t)slot * P->nrows;
+            int r2 = spmm_dispatch(P, k, EDX_C128, V, k, out, 1, depth * P->nrows,
                                    make_double2(1, 0), make_double2(0, 0), make_double2(0, 0), 0, st);
             if (r2) return r2;
             if (i > 0) {  // the stored vectors are unnormalised: scale to v_i
                 const int64_t tot = P->nrows * (int64_t)k;
                 const int blocks = (int)std::min<int64_t>((tot + 255) / 256, (int64_t)num_sms() * 8);
-                k_proj_scale<<<blocks, 256, 0, st>>>(P->nrows, k, maxn, i,
+                k_proj_scale<<<blocks, 256, 0, st>>>(P->nrows, k, depth, slot,
                                                      reinterpret_cast<double2*>(opts->proj_out[p]), ws.scur);
                 EDX_CHECK_LAUNCH();
             }
         }
+        if (win && ++win_n == win) return flush();
         return EDX_OK;
     };
     if ((rc = project(ws.Vc, 0))) return rc;
@@ -1044,6 +1088,10 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
             if (h[0] == 0) break;
             if (nshift > 0 && h[1] == 0) break;
         }
+    }
+    if ((rc = flush())) {
+        drop_events();
+        return rc;
     }
     if (nshift > 0) {
         k_shift_final<<<(nshift + 127) / 128, 128, 0, st>>>(nshift, ws.sst, opts->shift_iters, opts->shift_res);

@@ -7,6 +7,8 @@
 // each loaded once, with L1 no-allocate / L2 evict-first hints since the matrix is read
 // once per product) while the gathered X rows stay L2-resident.  Column tiles of width KW
 // run as grid.y so that wide blocks (k = 768) keep one X tile hot in L2 at a time.
+#include <algorithm>
+
 #include "edx_spmm.cuh"
 
 namespace edx {
@@ -196,6 +198,98 @@ int spmm_dispatch(const edx_csr* A, int k, int vec_type, const void* x, int64_t 
     return launch_spmm_v<float2, float2>(A, k, kw, x, ldx_, y, ldy, ycs, al, sg, be, st);
 }
 
+// ---- the same product on the packed form ----------------------------------------------
+// Warp per row (slots of KW lanes share the row's entries), value table in shared memory,
+// diagonal term added with the store.
+template <int KW, bool WIDE>
+__global__ void __launch_bounds__(256) k_spmm_packed(int64_t nrows, PackedView M, int k, const double2* __restrict__ X,
+                                                     int64_t ldx_, double2* __restrict__ Y, int64_t ldy,
+                                                     double2 alpha, double2 sigma, double2 beta, int has_sigma,
+                                                     int has_beta) {
+    extern __shared__ double2 sp_tab[];
+    for (int i = threadIdx.x; i < M.nval; i += blockDim.x) sp_tab[i] = M.vals[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int c = lane % KW;
+    const int col0 = blockIdx.y * KW;
+    const int gc = col0 + c;
+    const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    auto store = [&](int64_t r, double2 acc) {
+        const double2 xr = X[r * ldx_ + gc];
+        const double2 a = fma_c(__ldg(M.diag + r), xr, acc);
+        double yr = alpha.x * a.x - alpha.y * a.y;
+        double yi = alpha.x * a.y + alpha.y * a.x;
+        if (has_sigma) {
+            yr += sigma.x * xr.x - sigma.y * xr.y;
+            yi += sigma.x * xr.y + sigma.y * xr.x;
+        }
+        double2* yp = Y + r * ldy + gc;
+        if (has_beta) {
+            const double2 yv = *yp;
+            yr += beta.x * yv.x - beta.y * yv.y;
+            yi += beta.x * yv.y + beta.y * yv.x;
+        }
+        *yp = make_double2(yr, yi);
+    };
+    if (KW == 1) {  // one column: the next row's words load during this row
+        spmv_rows_packed<WIDE>(warp0, nrows, nw, M, sp_tab, X, ldx_, col0, [&](int64_t r, double2 acc) {
+            if (lane == 0) store(r, acc);
+        });
+        return;
+    }
+    for (int64_t r = warp0; r < nrows; r += nw) {
+        const int64_t s = __ldg(M.row_ptr + r), e = __ldg(M.row_ptr + r + 1);
+        double2 acc[1];
+        row_times_x_packed<KW, 1, WIDE>(s, e, M.ent, M.vidx, M.vbits, sp_tab, X, ldx_, col0, k, acc);
+        if (lane < KW && gc < k) store(r, acc[0]);
+    }
+}
+
+template <int KW, bool WIDE>
+static int launch_spmm_packed_t(const PackedView& M, int64_t n, int k, const double2* x, int64_t ldx_, double2* y,
+                                int64_t ldy, double2 al, double2 sg, double2 be, cudaStream_t st) {
+    const int threads = 256;
+    const size_t smem = (size_t)M.nval * sizeof(double2);
+    static int cache[EDX_MAX_DEVICES] = {};
+    int dev = 0;
+    EDX_CUDA(cudaGetDevice(&dev));
+    EDX_REQUIRE(dev >= 0 && dev < EDX_MAX_DEVICES, "edx_spmm_packed: device ordinal %d out of range", dev);
+    if (cache[dev] == 0) {  // resident blocks with the largest table
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_spmm_packed<KW, WIDE>, threads,
+                                                          EDX_PACK_VALUES_MAX * sizeof(double2)) != cudaSuccess ||
+            nb < 1)
+            nb = 4;
+        cache[dev] = nb;
+    }
+    const int64_t need = (n * 32 + threads - 1) / threads;
+    const int64_t maxb = (int64_t)num_sms() * cache[dev];
+    const int64_t bx = std::max<int64_t>(1, std::min(need, maxb));
+    dim3 grid((unsigned)bx, (unsigned)((k + KW - 1) / KW));
+    const int hs = (sg.x != 0.0 || sg.y != 0.0) ? 1 : 0;
+    const int hb = (be.x != 0.0 || be.y != 0.0) ? 1 : 0;
+    k_spmm_packed<KW, WIDE><<<grid, threads, smem, st>>>(n, M, k, x, ldx_, y, ldy, al, sg, be, hs, hb);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}
+
+template <bool WIDE>
+static int launch_spmm_packed(const PackedView& M, int64_t n, int k, int kw, const double2* x, int64_t ldx_,
+                              double2* y, int64_t ldy, double2 al, double2 sg, double2 be, cudaStream_t st) {
+    switch (kw) {
+    case 1: return launch_spmm_packed_t<1, WIDE>(M, n, k, x, ldx_, y, ldy, al, sg, be, st);
+    case 2: return launch_spmm_packed_t<2, WIDE>(M, n, k, x, ldx_, y, ldy, al, sg, be, st);
+    case 4: return launch_spmm_packed_t<4, WIDE>(M, n, k, x, ldx_, y, ldy, al, sg, be, st);
+    case 6: return launch_spmm_packed_t<6, WIDE>(M, n, k, x, ldx_, y, ldy, al, sg, be, st);
+    case 8: return launch_spmm_packed_t<8, WIDE>(M, n, k, x, ldx_, y, ldy, al, sg, be, st);
+    case 12: return launch_spmm_packed_t<12, WIDE>(M, n, k, x, ldx_, y, ldy, al, sg, be, st);
+    case 16: return launch_spmm_packed_t<16, WIDE>(M, n, k, x, ldx_, y, ldy, al, sg, be, st);
+    case 32: return launch_spmm_packed_t<32, WIDE>(M, n, k, x, ldx_, y, ldy, al, sg, be, st);
+    }
+    return fail(EDX_ERR_INVALID, "edx_spmm_packed: unsupported column group width %d", kw);
+}
+
 }  // namespace edx
 
 using namespace edx;
@@ -218,4 +312,31 @@ extern "C" int edx_spmm(const edx_csr* A, int k, int vec_type, const void* d_x, 
     return spmm_dispatch(A, k, vec_type, d_x, ldx_, d_y, ldy, 1, make_double2(alpha_re, alpha_im),
                          make_double2(sigma_re, sigma_im), make_double2(beta_re, beta_im), col_group,
                          as_stream(stream));
+}
+
+extern "C" int edx_spmm_packed(const edx_packed* P, int k, const double* d_x, int64_t ldx_, double* d_y, int64_t ldy,
+                               double alpha_re, double alpha_im, double sigma_re, double sigma_im, double beta_re,
+                               double beta_im, int col_group, void* stream) {
+    EDX_REQUIRE(P != nullptr && P->nrows >= 0 && P->nnz >= 0, "edx_spmm_packed: bad matrix");
+    EDX_REQUIRE(P->nrows == 0 || (P->row_ptr && P->diag), "edx_spmm_packed: matrix without row pointers");
+    EDX_REQUIRE(P->nnz == 0 || (P->ent && P->vals && P->nval >= 1), "edx_spmm_packed: matrix without entries");
+    EDX_REQUIRE(P->nval >= 0 && P->nval <= EDX_PACK_VALUES_MAX && P->vbits >= 0 && P->vbits <= 31,
+                "edx_spmm_packed: bad value table");
+    EDX_REQUIRE(P->vbits > 0 || P->nnz == 0 || P->vidx, "edx_spmm_packed: the wide form needs vidx");
+    EDX_REQUIRE(k >= 1, "edx_spmm_packed: k must be >= 1");
+    EDX_REQUIRE(ldx_ >= k && ldy >= k, "edx_spmm_packed: leading dimensions must be >= k");
+    EDX_REQUIRE(d_x != nullptr && d_y != nullptr, "edx_spmm_packed: NULL vectors");
+    EDX_REQUIRE(col_group == 0 || col_group == 1 || col_group == 2 || col_group == 4 || col_group == 6 ||
+                    col_group == 8 || col_group == 12 || col_group == 16 || col_group == 32,
+                "edx_spmm_packed: column group width must be one of 1, 2, 4, 6, 8, 12, 16, 32");
+    if (P->nrows == 0) return EDX_OK;
+    const int kw = col_group > 0 ? col_group : auto_kw(k);
+    const PackedView M{P->row_ptr, P->ent, reinterpret_cast<const double2*>(P->vals),
+                       reinterpret_cast<const double2*>(P->diag), P->vbits, P->nval, P->vidx};
+    const double2 al = make_double2(alpha_re, alpha_im), sg = make_double2(sigma_re, sigma_im),
+                  be = make_double2(beta_re, beta_im);
+    const double2* x = reinterpret_cast<const double2*>(d_x);
+    double2* y = reinterpret_cast<double2*>(d_y);
+    if (P->vbits == 0) return launch_spmm_packed<true>(M, P->nrows, k, kw, x, ldx_, y, ldy, al, sg, be, as_stream(stream));
+    return launch_spmm_packed<false>(M, P->nrows, k, kw, x, ldx_, y, ldy, al, sg, be, as_stream(stream));
 }

@@ -257,22 +257,128 @@ __device__ __forceinline__ uint32_t ld_stream1(const uint32_t* p) {
     return v;
 }
 
-// Off-diagonal part of row r of a packed matrix (word = column << vbits | value index; values
-// in the shared-memory table `tab`) times TG column tiles of X.  Same lane layout and result
-// as row_times_x_tiles.  With one slot per warp (KW = 32) every lane walks the same entries,
-// four words per 16-byte broadcast load, so an entry costs one table read and no shuffles.
-// With several slots, slot s takes entries start + s, start + s + SLOTS, ...; one load
-// instruction fetches adjacent words for all slots.
-template <int KW, int TG>
+// device view of an edx_packed matrix
+struct PackedView {
+    const int64_t* row_ptr;
+    const uint32_t* ent;
+    const double2* vals;
+    const double2* diag;
+    int vbits, nval;
+    const uint16_t* vidx;  // wide form (vbits == 0)
+};
+
+// 16-bit value indices of the wide packed form, streamed like the entry words
+__device__ __forceinline__ uint32_t ld_stream_u16(const uint16_t* p) {
+    unsigned short v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;"
+                 : "=h"(v)
+                 : "l"(p), "l"(evict_first_policy()));
+    return v;
+}
+__device__ __forceinline__ uint2 ld_stream_u16x4(const uint16_t* p) {  // 4 indices, 8-byte aligned
+    uint2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+                 : "=r"(v.x), "=r"(v.y)
+                 : "l"(p), "l"(evict_first_policy()));
+    return v;
+}
+
+// column and value index of one packed entry: narrow form w = column << vbits | index;
+// wide form (WIDE) w = column, vi = index
+template <bool WIDE>
+__device__ __forceinline__ void pk_decode(uint32_t w, uint32_t vi, int vbits, uint32_t vmask, int64_t& col,
+                                          uint32_t& idx) {
+    if (WIDE) {
+        col = (int64_t)w;
+        idx = vi;
+    } else {
+        col = (int64_t)(w >> vbits);
+        idx = w & vmask;
+    }
+}
+
+// One-column product on the packed form, warp per row, as spmv_rows: lanes take entries
+// lane, lane + 32, ... (coalesced word loads), the next row's first 128 words load while this
+// row's gathers run, the value comes from the shared-memory table `tab`.
+template <bool WIDE, class Epi>
+__device__ __forceinline__ void spmv_rows_packed(int64_t r0, int64_t r1, int64_t rstep, const PackedView& M,
+                                                 const double2* tab, const double2* __restrict__ X, int64_t ldx_,
+                                                 int col0, Epi epi) {
+    const int lane = threadIdx.x & 31;
+    if (r0 >= r1) return;
+    const uint32_t vmask = WIDE ? 0u : (1u << M.vbits) - 1u;
+    uint32_t ww[4], wi[4];
+    int64_t s = __ldg(M.row_ptr + r0), e = __ldg(M.row_ptr + r0 + 1);
+    auto load4 = [&](int64_t st, int64_t en, uint32_t* w4, uint32_t* i4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t j = st + u * 32 + lane;
+            w4[u] = j < en ? ld_stream1(M.ent + j) : 0u;
+            i4[u] = (WIDE && j < en) ? ld_stream_u16(M.vidx + j) : 0u;
+        }
+    };
+    load4(s, e, ww, wi);
+    for (int64_t r = r0; r < r1; r += rstep) {
+        const int64_t rn = r + rstep;
+        int64_t sn = 0, en = 0;
+        uint32_t wn[4], in_[4];
+        if (rn < r1) {
+            sn = __ldg(M.row_ptr + rn);
+            en = __ldg(M.row_ptr + rn + 1);
+        }
+        load4(sn, en, wn, in_);
+        double2 acc = make_double2(0.0, 0.0);
+        double2 xs[4], vs[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            int64_t cc;
+            uint32_t q;
+            pk_decode<WIDE>(ww[u], wi[u], M.vbits, vmask, cc, q);
+            const bool ok = s + u * 32 + lane < e;
+            xs[u] = ok ? ldx(X + cc * ldx_ + col0) : make_double2(0.0, 0.0);
+            vs[u] = ok ? tab[q] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc = fma_c(vs[u], xs[u], acc);
+        for (int64_t base = s + 128; base < e; base += 32) {  // tail of a long row
+            const int64_t j = base + lane;
+            if (j < e) {
+                int64_t cc;
+                uint32_t q;
+                pk_decode<WIDE>(ld_stream1(M.ent + j), WIDE ? ld_stream_u16(M.vidx + j) : 0u, M.vbits, vmask, cc, q);
+                acc = fma_c(tab[q], ldx(X + cc * ldx_ + col0), acc);
+            }
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) acc = xor_sum(acc, off);
+        epi(r, acc);
+        s = sn;
+        e = en;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            ww[u] = wn[u];
+            wi[u] = in_[u];
+        }
+    }
+}
+
+// Off-diagonal part of row r of a packed matrix (values in the shared-memory table `tab`)
+// times TG column tiles of X.  Same lane layout and result as row_times_x_tiles.  With one
+// slot per warp (KW = 32) every lane walks the same entries, four words per 16-byte broadcast
+// load (and four wide-form indices per 8-byte load), so an entry costs one table read and no
+// shuffles.  With several slots, slot s takes entries start + s, start + s + SLOTS, ...; one
+// load instruction fetches adjacent words for all slots.
+template <int KW, int TG, bool WIDE>
 __device__ __forceinline__ void row_times_x_packed(int64_t start, int64_t end, const uint32_t* __restrict__ ent,
-                                                   int vbits, const double2* tab, const double2* __restrict__ X,
-                                                   int64_t ldx_, int col0, int k, double2* acc) {
+                                                   const uint16_t* __restrict__ vidx, int vbits, const double2* tab,
+                                                   const double2* __restrict__ X, int64_t ldx_, int col0, int k,
+                                                   double2* acc) {
     constexpr int SLOTS = Slots<KW>::N;
     const int lane = threadIdx.x & 31;
     const int slot = lane / KW;
     const int c = lane % KW;
     const bool slot_ok = slot < SLOTS;
-    const uint32_t vmask = (1u << vbits) - 1u;
+    const uint32_t vmask = WIDE ? 0u : (1u << vbits) - 1u;
     bool colok[TG];
 #pragma unroll
     for (int g = 0; g < TG; ++g) {
@@ -280,23 +386,35 @@ __device__ __forceinline__ void row_times_x_packed(int64_t start, int64_t end, c
         acc[g] = make_double2(0.0, 0.0);
     }
     if (SLOTS == 1) {
-        auto one = [&](uint32_t w) {
-            const double2 v = tab[w & vmask];
-            const int64_t cc = (int64_t)(w >> vbits);
+        auto one = [&](int64_t j) {
+            int64_t cc;
+            uint32_t vi;
+            pk_decode<WIDE>(ld_stream1(ent + j), WIDE ? ld_stream_u16(vidx + j) : 0u, vbits, vmask, cc, vi);
+            const double2 v = tab[vi];
 #pragma unroll
             for (int g = 0; g < TG; ++g)
                 if (colok[g]) acc[g] = fma_c(v, ldx(X + cc * ldx_ + col0 + g * KW + c), acc[g]);
         };
         int64_t j = start;
-        for (; j < end && (j & 3); ++j) one(ld_stream1(ent + j));
+        for (; j < end && (j & 3); ++j) one(j);
         for (; j + 4 <= end; j += 4) {
             const uint4 w4 = ld_stream4(ent + j);
             const uint32_t w[4] = {w4.x, w4.y, w4.z, w4.w};
+            uint32_t vi[4] = {0u, 0u, 0u, 0u};
+            if (WIDE) {
+                const uint2 i4 = ld_stream_u16x4(vidx + j);
+                vi[0] = i4.x & 0xffffu;
+                vi[1] = i4.x >> 16;
+                vi[2] = i4.y & 0xffffu;
+                vi[3] = i4.y >> 16;
+            }
             double2 v[4], xs[4][TG];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                v[u] = tab[w[u] & vmask];
-                const int64_t cc = (int64_t)(w[u] >> vbits);
+                int64_t cc;
+                uint32_t q;
+                pk_decode<WIDE>(w[u], vi[u], vbits, vmask, cc, q);
+                v[u] = tab[q];
 #pragma unroll
                 for (int g = 0; g < TG; ++g)
                     xs[u][g] = colok[g] ? ldx(X + cc * ldx_ + col0 + g * KW + c) : make_double2(0.0, 0.0);
@@ -306,32 +424,39 @@ __device__ __forceinline__ void row_times_x_packed(int64_t start, int64_t end, c
 #pragma unroll
                 for (int g = 0; g < TG; ++g) acc[g] = fma_c(v[u], xs[u][g], acc[g]);
         }
-        for (; j < end; ++j) one(ld_stream1(ent + j));
+        for (; j < end; ++j) one(j);
     } else {
         constexpr int U = 4;
         // words of the next U groups load while this batch's gathers run
-        uint32_t nw[U];
+        uint32_t nw[U], ni[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const int64_t j = start + (int64_t)u * SLOTS + slot;
-            nw[u] = (slot_ok && j < end) ? ld_stream1(ent + j) : 0u;
+            const bool ok = slot_ok && j < end;
+            nw[u] = ok ? ld_stream1(ent + j) : 0u;
+            ni[u] = (WIDE && ok) ? ld_stream_u16(vidx + j) : 0u;
         }
         for (int64_t base = start; base < end; base += (int64_t)SLOTS * U) {
-            uint32_t w[U];
+            uint32_t w[U], wi[U];
             bool ok[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int64_t j = base + (int64_t)u * SLOTS + slot;
                 ok[u] = slot_ok && j < end;
                 w[u] = nw[u];
+                wi[u] = ni[u];
                 const int64_t jn = j + (int64_t)SLOTS * U;
-                nw[u] = (slot_ok && jn < end) ? ld_stream1(ent + jn) : 0u;
+                const bool okn = slot_ok && jn < end;
+                nw[u] = okn ? ld_stream1(ent + jn) : 0u;
+                ni[u] = (WIDE && okn) ? ld_stream_u16(vidx + jn) : 0u;
             }
             double2 v[U], xs[U][TG];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                v[u] = ok[u] ? tab[w[u] & vmask] : make_double2(0.0, 0.0);
-                const int64_t cc = (int64_t)(w[u] >> vbits);
+                int64_t cc;
+                uint32_t q;
+                pk_decode<WIDE>(w[u], wi[u], vbits, vmask, cc, q);
+                v[u] = ok[u] ? tab[q] : make_double2(0.0, 0.0);
 #pragma unroll
                 for (int g = 0; g < TG; ++g)
                     xs[u][g] = (ok[u] && colok[g]) ? ldx(X + cc * ldx_ + col0 + g * KW + c) : make_double2(0.0, 0.0);

@@ -98,7 +98,7 @@ def basis_from_states(states):
 class CSR:
     row_ptr: torch.Tensor          # int64 [nrows+1]
     col: torch.Tensor              # int32 [nnz]
-    val: torch.Tensor              # complex128 [nnz]
+    val: Optional[torch.Tensor]    # complex128 [nnz] (None for a complex64-only matrix)
     ncols: int
     val64: Optional[torch.Tensor] = None  # complex64 copy (mixed-precision products)
 
@@ -114,15 +114,23 @@ class CSR:
         v = self.val64 if c64 else self.val
         if c64 and v is None:
             raise ValueError("this CSR has no complex64 copy")
+        if not c64 and v is None:
+            raise ValueError("this CSR holds complex64 values only (use c64=True)")
         return Csr(self.nrows, self.ncols, self.nnz, _ptr(self.row_ptr), _ptr(self.col), _ptr(v),
                    C64 if c64 else C128)
 
     def nbytes(self, c64=False):
         return self.row_ptr.numel() * 8 + self.nnz * (4 + (8 if c64 else 16))
 
-    def to_c64(self):
+    def to_c64(self, drop_c128=False, chunk=1 << 28):
+        """Add the complex64 copy (converted in chunks, so the peak is the two arrays plus one
+        chunk); drop_c128 then releases the complex128 values."""
         if self.val64 is None:
-            self.val64 = self.val.to(torch.complex64)
+            self.val64 = torch.empty(self.val.numel(), dtype=torch.complex64, device=self.val.device)
+            for a in range(0, self.val.numel(), chunk):
+                self.val64[a:a + chunk].copy_(self.val[a:a + chunk])
+        if drop_c128:
+            self.val = None
         return self
 
 
@@ -136,9 +144,14 @@ def _terms_to_device(terms, nidx):
 
 
 def build_csr(mode, left: Basis, hopping, coulomb=None, right: Optional[Basis] = None, num_val_orbs=0,
-              num_core_orbs=0, ham_sign=1.0, omega=0j, want_c64=False):
+              num_core_orbs=0, ham_sign=1.0, omega=0j, want_c64=False, values=None):
     """Two-pass CSR build of src/ham.f90 (see include/edx.h).  hopping/coulomb are
-    (idx 1-based, values) pairs as read from the *.in files."""
+    (idx 1-based, values) pairs as read from the *.in files.  values: "c128" (default),
+    "both" (also a complex64 copy; want_c64=True means the same) or "c64" (complex64 only,
+    for matrices too large to hold in complex128)."""
+    values = values or ("both" if want_c64 else "c128")
+    if values not in ("c128", "c64", "both"):
+        raise ValueError("build_csr: values must be c128, c64 or both")
     require_cuda()
     hi, hv, nh = _terms_to_device(hopping, 2)
     ci, cv, ncl = _terms_to_device(coulomb, 4)
@@ -164,8 +177,10 @@ def build_csr(mode, left: Basis, hopping, coulomb=None, right: Optional[Basis] =
     call("edx_build_scan", _ptr(row_nnz), nrows, _ptr(row_ptr), ctypes.byref(nnz), _ptr(w), sws.value, st)
     del row_nnz
     col = torch.empty(max(nnz.value, 1), dtype=torch.int32, device="cuda")[:nnz.value]
-    val = torch.empty(max(nnz.value, 1), dtype=torch.complex128, device="cuda")[:nnz.value]
-    val64 = torch.empty(max(nnz.value, 1), dtype=torch.complex64, device="cuda")[:nnz.value] if want_c64 else None
+    val = torch.empty(max(nnz.value, 1), dtype=torch.complex128, device="cuda")[:nnz.value] \
+        if values != "c64" else None
+    val64 = torch.empty(max(nnz.value, 1), dtype=torch.complex64, device="cuda")[:nnz.value] \
+        if values != "c128" else None
     if nnz.value > 0:
         call("edx_build_fill", ctypes.byref(d), cap.value, _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(val64),
              _ptr(w), ws.value, st)
@@ -273,31 +288,56 @@ PACK_VALUES_MAX = 2048
 class PackedMatrix:
     """Device arrays of an edx_packed matrix (see include/edx.h); keeps them alive."""
     row_ptr: torch.Tensor   # int64 [n+1], off-diagonal entries
-    ent: torch.Tensor       # int32 [nnz] holding the uint32 words column << vbits | value index
+    ent: torch.Tensor       # int32 [nnz]: uint32 words column << vbits | value index (narrow),
+                            # or the column (wide, vbits == 0)
     vals: torch.Tensor      # complex128 [nval]
     diag: torch.Tensor      # complex128 [n]
     vbits: int
+    vidx: Optional[torch.Tensor] = None  # int16 [nnz] holding uint16 value indices (wide form)
 
     @property
     def nrows(self):
         return self.row_ptr.numel() - 1
 
+    ncols = nrows
+
+    @property
+    def nnz(self):
+        return self.ent.numel()
+
+    @property
+    def wide(self):
+        return self.vbits == 0
+
     def desc(self):
         return Packed(self.nrows, self.ent.numel(), _ptr(self.row_ptr), _ptr(self.ent), self.vbits,
-                      self.vals.numel(), _ptr(self.vals), _ptr(self.diag))
+                      self.vals.numel(), _ptr(self.vals), _ptr(self.diag),
+                      _ptr(self.vidx) if self.vidx is not None else None)
+
+    def shape_desc(self):
+        """A CSR descriptor with this matrix's shape and no entries, for calls whose product
+        runs on the packed form (edx_krylov with apply_packed)."""
+        return Csr(self.nrows, self.nrows, 0, _ptr(self.row_ptr), None, None, C128)
 
     def nbytes(self):
-        return sum(t.numel() * t.element_size() for t in (self.row_ptr, self.ent, self.vals, self.diag))
+        ts = [self.row_ptr, self.ent, self.vals, self.diag] + ([self.vidx] if self.vidx is not None else [])
+        return sum(t.numel() * t.element_size() for t in ts)
 
     def unpack(self):
         """(row_ptr, col, val) of the off-diagonal entries, for checks."""
         w = self.ent.to(torch.int64) & 0xFFFFFFFF
+        if self.wide:
+            return self.row_ptr, w, self.vals[self.vidx.to(torch.int64) & 0xFFFF]
         return self.row_ptr, (w >> self.vbits), self.vals[w & ((1 << self.vbits) - 1)]
 
 
-def pack(A: CSR):
+PACK_FORMS = {"auto": 0, "narrow": 1, "wide": 2}
+
+
+def pack(A: CSR, form="auto"):
     """Packed form of the square complex128 matrix A, or None when A has more distinct
-    off-diagonal values than a 32-bit entry word can index."""
+    off-diagonal values than the form can index.  form: "auto" (the 32-bit word when the
+    column leaves room for the value index, else the wide form), "narrow" or "wide"."""
     require_cuda()
     d = A.desc()
     ws = ctypes.c_size_t(0)
@@ -306,17 +346,19 @@ def pack(A: CSR):
     nnz, nval, vbits = ctypes.c_int64(0), ctypes.c_int(0), ctypes.c_int(0)
     st = _stream()
     try:
-        call("edx_pack_count", ctypes.byref(d), ctypes.byref(nnz), ctypes.byref(nval), ctypes.byref(vbits),
-             _ptr(w), ws.value, st)
+        call("edx_pack_count", ctypes.byref(d), PACK_FORMS[form], ctypes.byref(nnz), ctypes.byref(nval),
+             ctypes.byref(vbits), _ptr(w), ws.value, st)
     except _lib.EdxError as e:
         if e.code == 5:  # EDX_ERR_OVERFLOW: too many distinct values
             return None
         raise
     n = A.nrows
+    m = nnz.value
     P = PackedMatrix(torch.empty(n + 1, dtype=torch.int64, device="cuda"),
-                     torch.empty(max(nnz.value, 1), dtype=torch.int32, device="cuda")[:nnz.value],
+                     torch.empty(max(m, 1), dtype=torch.int32, device="cuda")[:m],
                      torch.empty(max(nval.value, 1), dtype=torch.complex128, device="cuda")[:nval.value],
-                     torch.empty(n, dtype=torch.complex128, device="cuda"), vbits.value)
+                     torch.empty(n, dtype=torch.complex128, device="cuda"), vbits.value,
+                     torch.empty(max(m, 1), dtype=torch.int16, device="cuda")[:m] if vbits.value == 0 else None)
     t = P.desc()
     call("edx_pack_fill", ctypes.byref(d), ctypes.byref(t), _ptr(w), ws.value, st)
     return P
@@ -326,8 +368,9 @@ def pack(A: CSR):
 # products and solvers
 # ------------------------------------------------------------------------------------
 
-def spmm(A: CSR, X, Y=None, alpha=1.0, sigma=0.0, beta=0.0, c64=False, col_group=0):
-    """Y = alpha*(A X) + sigma*X + beta*Y; X is (ncols,) or (ncols, k) row-major."""
+def spmm(A, X, Y=None, alpha=1.0, sigma=0.0, beta=0.0, c64=False, col_group=0):
+    """Y = alpha*(A X) + sigma*X + beta*Y; X is (ncols,) or (ncols, k) row-major.  A is a CSR
+    or a PackedMatrix (edx_spmm_packed)."""
     squeeze = X.dim() == 1
     Xm = X.reshape(X.shape[0], -1)
     k = Xm.shape[1]
@@ -343,8 +386,14 @@ def spmm(A: CSR, X, Y=None, alpha=1.0, sigma=0.0, beta=0.0, c64=False, col_group
     if k > 1 and Ym.stride(1) != 1:
         raise ValueError("spmm: Y must be row-major (n, k)")
     al, sg, be = complex(alpha), complex(sigma), complex(beta)
-    call("edx_spmm", ctypes.byref(A.desc(c64)), k, vec_type, _ptr(Xm), Xm.stride(0), _ptr(Ym), Ym.stride(0),
-         al.real, al.imag, sg.real, sg.imag, be.real, be.imag, col_group, _stream())
+    if isinstance(A, PackedMatrix):
+        if vec_type != C128 or c64:
+            raise ValueError("spmm: a packed matrix takes complex128 vectors")
+        call("edx_spmm_packed", ctypes.byref(A.desc()), k, _ptr(Xm), Xm.stride(0), _ptr(Ym), Ym.stride(0),
+             al.real, al.imag, sg.real, sg.imag, be.real, be.imag, col_group, _stream())
+    else:
+        call("edx_spmm", ctypes.byref(A.desc(c64)), k, vec_type, _ptr(Xm), Xm.stride(0), _ptr(Ym), Ym.stride(0),
+             al.real, al.imag, sg.real, sg.imag, be.real, be.imag, col_group, _stream())
     return Y.reshape(-1) if squeeze else Y
 
 
@@ -360,11 +409,20 @@ class KrylovResult:
     shift_res: Optional[torch.Tensor] = None
 
 
-def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_maxit=None, timing=False,
-           apply=None):
+def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_maxit=None, timing=False,
+           apply=None, accumulate=None):
     """k independent Lanczos recurrences (build_krylov_mp) from the columns of V0 (n, k).
     proj: CSR operators applied to every Lanczos vector.  shifts: (col_index int array,
-    complex z array) -> per-shift MINRES coefficients in the Lanczos basis."""
+    complex z array) -> per-shift MINRES coefficients in the Lanczos basis.  A may be a
+    PackedMatrix: the product then runs on it and no CSR is needed.
+    accumulate: dict(window=B, col=(nacc,) ints, coef=(nacc, maxn) complex128 device tensor,
+    out=[one (nrows_p, nacc) row-major view per projector]) -> instead of storing every
+    projected vector, out[p][:, s] += sum_i coef[s, i] * (proj[p] v_i)[:, col[s]], keeping
+    only the last B projected vectors."""
+    if isinstance(A, PackedMatrix):
+        apply = dict(apply or {}, packed=A)
+        if apply.get("layout") is not None:
+            raise ValueError("krylov: a packed matrix has no tiled layout")
     V0 = V0.reshape(V0.shape[0], -1).contiguous()
     n, k = V0.shape
     dev = V0.device
@@ -376,13 +434,36 @@ def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, s
     keep = []
     outs = []
     if proj:
+        depth = int(accumulate["window"]) if accumulate else maxn
         descs = (Csr * len(proj))(*[P.desc() for P in proj])
-        outs = [torch.zeros((k, maxn, P.nrows), dtype=torch.complex128, device=dev) for P in proj]
+        outs = [torch.zeros((k, depth, P.nrows), dtype=torch.complex128, device=dev) for P in proj]
         ptrs = (ctypes.c_void_p * len(proj))(*[o.data_ptr() for o in outs])
         opts.nproj = len(proj)
         opts.proj = descs
         opts.proj_out = ptrs
         keep += [descs, ptrs]
+        if accumulate:
+            acc_col = torch.as_tensor(np.asarray(accumulate["col"], dtype=np.int32), device=dev)
+            coef = accumulate["coef"]
+            aouts = accumulate["out"]
+            nacc = acc_col.numel()
+            if coef.dtype != torch.complex128 or tuple(coef.shape) != (nacc, maxn) or not coef.is_contiguous():
+                raise ValueError("krylov: accumulate coef must be a contiguous (nacc, maxn) complex128 tensor")
+            if len(aouts) != len(proj):
+                raise ValueError("krylov: one accumulator block per projector")
+            ld = aouts[0].stride(0)
+            for P, o in zip(proj, aouts):
+                if o.dtype != torch.complex128 or tuple(o.shape) != (P.nrows, nacc) or o.stride(1) != 1 \
+                        or o.stride(0) != ld:
+                    raise ValueError("krylov: accumulator blocks must be (nrows_p, nacc) row-major views, one ld")
+            aptrs = (ctypes.c_void_p * len(proj))(*[o.data_ptr() for o in aouts])
+            opts.proj_window = depth
+            opts.nacc = nacc
+            opts.acc_col = _ptr(acc_col)
+            opts.acc_coef = _ptr(coef)
+            opts.acc_out = aptrs
+            opts.acc_ld = ld
+            keep += [acc_col, aptrs]
     sy = si = sr = None
     if shifts is not None:
         scol, sz = shifts
@@ -424,9 +505,10 @@ def krylov(A: CSR, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, s
     ws = ctypes.c_size_t(0)
     call("edx_krylov_workspace", n, k, ctypes.byref(opts), maxn, ctypes.byref(ws))
     w = _work(ws.value)
-    call("edx_krylov", ctypes.byref(A.desc(c64)), k, _ptr(V0), maxn, _ptr(alpha), _ptr(beta), _ptr(norm),
+    adesc = A.shape_desc() if isinstance(A, PackedMatrix) else A.desc(c64)
+    call("edx_krylov", ctypes.byref(adesc), k, _ptr(V0), maxn, _ptr(alpha), _ptr(beta), _ptr(norm),
          _ptr(neff), ctypes.byref(opts), _ptr(w), ws.value, _stream())
-    res = KrylovResult(alpha, beta, norm, neff, outs, sy, si, sr)
+    res = KrylovResult(alpha, beta, norm, neff, [] if accumulate else outs, sy, si, sr)
     res.apply_ms = ms.value if timing else None
     res.apply_launches = nl.value
     return res

@@ -56,7 +56,8 @@ def _ed_core(cfg, H, basis):
         e, v = solvers.dense_eigs(H, max(neval, nvector))
         return e[:neval], v[:, :nvector]
     tol = min(float(cfg["eigval_tol"]), 1e-9)
-    e, v = solvers.lowest_eigs(H, neval, nvector, tol=tol)
+    # products on the packed form when H has few enough distinct values (lossless)
+    e, v = solvers.lowest_eigs(H, neval, nvector, tol=tol, packed=device.pack(H))
     return e, v
 
 

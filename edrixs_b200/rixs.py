@@ -88,35 +88,61 @@ class RixsResult:
     stats: dict = field(default_factory=dict)  # kernel launch counts and timings
 
 
+def _stream_needed(P, k, maxn):
+    """True when storing D_out^+ v_i for every Lanczos vector would take more than a third of
+    the free device memory (then the two-pass streaming form is used)."""
+    free, _ = torch.cuda.mem_get_info()
+    stored = sum(D.nrows for D in P.Dout) * k * maxn * 16
+    return stored > free / 3
+
+
 def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, linsys_tol=1e-10,
-                 linsys_max=1000, temperature=300.0, c64=False, final_block=None, timing=False, autotune=False):
+                 linsys_max=1000, temperature=300.0, c64=False, final_block=None, timing=False, autotune=False,
+                 stream=None, stream_window=8, seeds=None, c64_final=None):
+    """RIXS spectra of every (omega_in, pol_in, pol_out, gs) of one request.
+    stream: None (automatic), True or False -- whether D_out^+ v_i is folded into the
+    final-state start vectors as the Lanczos vectors appear (two passes over H_n) instead of
+    being stored for every v_i.  seeds: the block D_in(pol_in)|g> (n_n, npin * ngs), column
+    p_in * ngs + g, when the caller computed it already (P.Din is then not used).  c64: the
+    H_n products (MINRES part) in complex64; c64_final: the H_f products too (default: as c64)."""
+    c64_f = c64 if c64_final is None else bool(c64_final)
     omegas = np.asarray(omegas, dtype=np.float64)
     eloss = np.asarray(eloss, dtype=np.float64)
     n_om, ne = len(omegas), len(eloss)
-    npin, npout, ngs = len(P.Din), len(P.Dout), len(P.gs_e)
+    npout, ngs = len(P.Dout), len(P.gs_e)
+    npin = len(P.Din) if seeds is None else seeds.shape[1] // ngs
     k_hn = npin * ngs
     K_hf = npout * k_hn * n_om if final_block is None else int(final_block)
     if autotune:
         from . import tune
         P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64, layout=P.tiles.get("hn"),
                                                              packed=P.packed.get("hn"))
-        P.meta[("apply", "hf", K_hf, c64)] = tune.tune_apply(P.Hf, K_hf, c64=c64, layout=P.tiles.get("hf"),
-                                                             packed=P.packed.get("hf"))
+        P.meta[("apply", "hf", K_hf, c64_f)] = tune.tune_apply(P.Hf, K_hf, c64=c64_f, layout=P.tiles.get("hf"),
+                                                               packed=P.packed.get("hf"))
     cfg_hn = _apply_args(P.meta.get(("apply", "hn", k_hn, c64)), P.tiles.get("hn"), P.packed.get("hn"), c64)
-    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64)), P.tiles.get("hf"), P.packed.get("hf"), c64)
+    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64_f)), P.tiles.get("hf"), P.packed.get("hf"), c64_f)
     gam_c = np.broadcast_to(np.asarray(gamma_c, dtype=np.float64), (n_om,))
     dev = P.gs_v.device
     # 1. seeds (n_n, npin*ngs), column c = p_in*ngs + g
-    seeds = torch.cat([device.spmm(D, P.gs_v) for D in P.Din], dim=1).contiguous()
+    if seeds is None:
+        seeds = torch.cat([device.spmm(D, P.gs_v) for D in P.Din], dim=1).contiguous()
     k = seeds.shape[1]
     # 2. shifts: for every column its n_om incident energies
     scol = np.repeat(np.arange(k, dtype=np.int32), n_om)
     gsE = np.tile(P.gs_e, npin)
     sz = (omegas[None, :] + gsE[:, None] + 1j * gam_c[None, :]).reshape(-1)
     maxn = int(linsys_max)
+    if stream is None:
+        stream = _stream_needed(P, k, maxn)
+    nf = P.Dout[0].nrows
+    K = npout * k * n_om
     # 3. one Krylov space per seed + projections through every D_out^+
-    r = device.krylov(P.Hn, seeds, maxn, c64=c64, proj=P.Dout, shifts=(scol, sz), shift_tol=linsys_tol,
-                      shift_maxit=linsys_max, timing=timing, apply=cfg_hn)
+    if not stream:
+        r = device.krylov(P.Hn, seeds, maxn, c64=c64, proj=P.Dout, shifts=(scol, sz), shift_tol=linsys_tol,
+                          shift_maxit=linsys_max, timing=timing, apply=cfg_hn)
+    else:  # pass 1: the shifted recurrences alone
+        r = device.krylov(P.Hn, seeds, maxn, c64=c64, shifts=(scol, sz), shift_tol=linsys_tol,
+                          shift_maxit=linsys_max, timing=timing, apply=cfg_hn)
     steps = int(r.neff.max().item())
     m = max(int(r.shift_iters.max().item()), 1)
     iters = r.shift_iters.view(k, n_om).cpu().numpy()
@@ -125,19 +151,35 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     # libedx launches on H_n: 4 setup + the first projections, then per iteration apply, orth,
     # shift step and per emission operator a projection and its column scaling
     stats = dict(hn_iterations=it_n, hn_apply_ms=r.apply_ms, hn_nnz=P.Hn.nnz, hn_rows=P.Hn.nrows, k_hn=k,
-                 launches=len(P.Din) + 4 + npout + it_n * (3 + 2 * npout))
-    Y = r.shift_y.view(k, n_om, -1)[:, :, :m]                     # (k, n_om, m)
-    # phi[p_out][c, w, :] = sum_i Y[c, w, i] * (D_out^+ v_i)[:]
-    phis = []
-    for po in range(npout):
-        W = r.proj[po][:, :m, :]                                   # (k, m, n_f)
-        phis.append(torch.matmul(Y, W))                            # (k, n_om, n_f)
-    del r
-    Phi = torch.stack(phis, dim=0)                                 # (npout, k, n_om, n_f)
-    nf = Phi.shape[-1]
-    K = npout * k * n_om
-    V0 = Phi.reshape(K, nf).T.contiguous()                         # (n_f, K) row-major
-    del Phi, phis
+                 launches=npin + 4 + npout + it_n * (3 + 2 * npout), streamed=bool(stream))
+    if not stream:
+        Y = r.shift_y.view(k, n_om, -1)[:, :, :m]                 # (k, n_om, m)
+        # phi[p_out][c, w, :] = sum_i Y[c, w, i] * (D_out^+ v_i)[:]
+        phis = []
+        for po in range(npout):
+            W = r.proj[po][:, :m, :]                               # (k, m, n_f)
+            phis.append(torch.matmul(Y, W))                        # (k, n_om, n_f)
+        del r
+        Phi = torch.stack(phis, dim=0)                             # (npout, k, n_om, n_f)
+        V0 = Phi.reshape(K, nf).T.contiguous()                     # (n_f, K) row-major
+        del Phi, phis
+    else:
+        # pass 2: the same m Lanczos vectors again (deterministic reductions: the same
+        # vectors), each D_out^+ v_i folded into phi as it appears, B vectors at a time
+        Y = r.shift_y[:, :m].contiguous()                          # (k * n_om, m)
+        r1_ms = r.apply_ms
+        del r
+        V0 = torch.zeros((nf, K), dtype=torch.complex128, device=dev)
+        nacc = k * n_om
+        outs = [V0[:, po * nacc:(po + 1) * nacc] for po in range(npout)]
+        r2 = device.krylov(P.Hn, seeds, m, c64=c64, proj=P.Dout, timing=timing, apply=cfg_hn,
+                           accumulate=dict(window=int(stream_window), col=scol, coef=Y, out=outs))
+        stats["hn_iterations"] += r2.apply_launches
+        if timing:
+            stats["hn_apply_ms"] = (r1_ms or 0.0) + (r2.apply_ms or 0.0)
+        stats["launches"] += 4 + npout + r2.apply_launches * (2 + 2 * npout) + \
+            npout * ((m + int(stream_window) - 1) // int(stream_window))
+        del r2, Y
     # 4. final-state Lanczos, all pole sets as one block (optionally in chunks of columns)
     blk = K if final_block is None else int(final_block)
     A = torch.zeros((K, nkryl), dtype=torch.float64, device=dev)
@@ -147,7 +189,7 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     hf_ms, hf_it = 0.0, 0
     for s in range(0, K, blk):
         e = min(K, s + blk)
-        rf = device.krylov(P.Hf, V0[:, s:e].contiguous(), nkryl, c64=c64, timing=timing, apply=cfg_hf)
+        rf = device.krylov(P.Hf, V0[:, s:e].contiguous(), nkryl, c64=c64_f, timing=timing, apply=cfg_hf)
         A[s:e], B[s:e], NRM[s:e], NEFF[s:e] = rf.alpha, rf.beta, rf.norm, rf.neff
         hf_ms += rf.apply_ms or 0.0
         hf_it += rf.apply_launches

@@ -108,14 +108,14 @@ class Resident:
                                            num_val_orbs=s.nv)
                 self.packed["hi"] = device.pack(self.Hi)
             if self.gs_v is None or self.gs_v.shape[1] < ngs:
-                e, v = solvers.lowest_eigs(self.Hi, ngs, ngs, tol=1e-9)
+                e, v = solvers.lowest_eigs(self.Hi, ngs, ngs, tol=1e-9, packed=self.packed.get("hi"))
                 self.gs_e, self.gs_v = np.asarray(e), v.contiguous()
             if need_n and self.Hn is None:
                 self.bn = device.fock_unrank(s.nv, s.nelec + 1)
                 self.Hn = device.build_csr(device.HAM_N, self.bn, self.terms["hop_n"], self.terms["coul_n"],
                                            num_val_orbs=s.nv, num_core_orbs=6)
                 self.packed["hn"] = device.pack(self.Hn)
-                e_n, _ = solvers.lowest_eigs(self.Hn, 1, 1, tol=1e-6)
+                e_n, _ = solvers.lowest_eigs(self.Hn, 1, 1, tol=1e-6, packed=self.packed.get("hn"))
                 self.edge = float(e_n[0] - self.gs_e[0])
             # the resident is shared with other workers' streams: finish building it here
             torch.cuda.current_stream().synchronize()

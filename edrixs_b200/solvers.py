@@ -4,7 +4,8 @@
 and the plain Lanczos of diag_ham_lanczos (src/lanczos.f90:6-167) with a block
 thick-restart Lanczos:
 
-* the Krylov block is expanded by one SpMM of width b per step (libedx ``edx_spmm``);
+* the Krylov block is expanded by one SpMM of width b per step (libedx ``edx_spmm``, or
+  ``edx_spmm_packed`` on the packed form of H);
 * every new block is orthogonalised against the whole basis twice (classical Gram-Schmidt,
   CGS2): tall-skinny contractions C = V^H W and W -= V^T C that libedx runs as single
   bandwidth-bound passes over the basis (``edx_gs_dot`` / ``edx_gs_update``), then the
@@ -63,8 +64,12 @@ def dense_eigs(H: device.CSR, nev):
 
 
 def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, max_restarts=200, seed=20240917,
-                c64=False, verbose=False):
-    """Lowest `nev` eigenvalues (ascending) and `nvec` eigenvectors (n, nvec) of Hermitian H."""
+                c64=False, verbose=False, packed=None):
+    """Lowest `nev` eigenvalues (ascending) and `nvec` eigenvectors (n, nvec) of Hermitian H.
+    packed: the packed form of H (device.pack); the block products then run on it.  H itself
+    may be a PackedMatrix when its CSR is no longer held."""
+    if isinstance(H, device.PackedMatrix):
+        packed = H
     n = H.nrows
     nvec = nev if nvec is None else nvec
     want = max(nev, nvec)
@@ -74,8 +79,10 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
         mmax = max(3 * want + 4 * b, 40)
     mmax = ((mmax + b - 1) // b) * b
     if n <= max(mmax + b, 64):
+        if isinstance(H, device.PackedMatrix):
+            raise ValueError("lowest_eigs: the dense solver of a small matrix needs its CSR")
         return dense_eigs(H, nev)[0], dense_eigs(H, nvec)[1]
-    dev = H.val.device
+    dev = torch.device("cuda", torch.cuda.current_device())
     dt = torch.complex128
     V = torch.zeros((mmax + b, n), dtype=dt, device=dev)  # basis vectors as rows
     T = np.zeros((mmax + b, mmax + b), dtype=np.complex128)
@@ -90,7 +97,7 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
     for restart in range(max_restarts):
         while j + b <= mmax:
             X = V[j:j + b].T.contiguous()
-            W = device.spmm(H, X, c64=c64).contiguous()
+            W = (device.spmm(packed, X) if packed is not None else device.spmm(H, X, c64=c64)).contiguous()
             # classical Gram-Schmidt twice against the whole basis (libedx: one pass over V each)
             C = device.gs_dot(V, j + b, W)
             device.gs_update(V, j + b, W, C)

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define EDX_ABI_VERSION 2
+#define EDX_ABI_VERSION 3
 
 /* status codes */
 #define EDX_OK 0
@@ -105,7 +105,8 @@ int edx_build_count(const edx_build_desc* d, int32_t* d_row_nnz, int* cap_out, v
 int edx_build_scan(const int32_t* d_row_nnz, int64_t nrows, int64_t* d_row_ptr, int64_t* h_nnz,
                    void* d_work, size_t work_bytes, void* stream);
 int edx_build_scan_workspace(int64_t nrows, size_t* bytes);
-/* Pass 2: columns and values at d_row_ptr[r]; d_val64 (complex64 copy) may be NULL. */
+/* Pass 2: columns and values at d_row_ptr[r]; d_val64 (complex64 copy) may be NULL, and
+ * d_val may be NULL when d_val64 is given (a complex64-only matrix). */
 int edx_build_fill(const edx_build_desc* d, int cap, const int64_t* d_row_ptr, int32_t* d_col,
                    double* d_val, float* d_val64, void* d_work, size_t work_bytes, void* stream);
 
@@ -187,30 +188,46 @@ int edx_tiles_fill(const edx_csr* A, edx_tiles* T, void* d_work, size_t work_byt
 /* A Hamiltonian built from a few hundred hopping and Coulomb terms has only a few hundred
  * distinct off-diagonal values (for example 418 in the 11.2 M entries of a 184,756-state
  * impurity model).  The packed form keeps the diagonal as a dense complex128 vector and
- * stores every off-diagonal entry as one 32-bit word:
- *   ent = column << vbits | index into vals (the distinct values, bit-exact copies),
- * with vbits = 32 - (bits of ncols-1).  Rows keep the CSR's column order.  The form exists
- * when nval <= min(2^vbits, EDX_PACK_VALUES_MAX). */
+ * stores every off-diagonal entry by its column and an index into vals (the distinct values,
+ * bit-exact copies).  Rows keep the CSR's column order.  Two forms:
+ *   narrow (vbits >= 1): one 32-bit word, ent = column << vbits | index, with
+ *     vbits = 32 - (bits of ncols-1); it exists when nval <= min(2^vbits, EDX_PACK_VALUES_MAX);
+ *   wide (vbits == 0): ent = column and vidx = index (16 bits), 6 bytes per entry, for
+ *     matrices whose column needs too many of the 32 bits (tens of millions of states);
+ *     it exists when nval <= EDX_PACK_VALUES_MAX. */
 #define EDX_PACK_VALUES_MAX 2048
+#define EDX_PACK_AUTO 0    /* narrow when it fits, else wide */
+#define EDX_PACK_NARROW 1
+#define EDX_PACK_WIDE 2
 typedef struct edx_packed {
     int64_t nrows;
     int64_t nnz;               /* off-diagonal entries */
     const int64_t* row_ptr;    /* device int64[nrows+1] */
     const uint32_t* ent;       /* device uint32[nnz] */
-    int vbits;
+    int vbits;                 /* 0: wide form */
     int nval;
     const double* vals;        /* device complex128[nval] */
     const double* diag;        /* device complex128[nrows]; zero where the CSR has no diagonal */
+    const uint16_t* vidx;      /* wide form: device uint16[nnz]; NULL for the narrow form */
 } edx_packed;
 
+/* The count pass sorts the off-diagonal values in chunks of at most 2^26 entries, so the
+ * workspace stays near 40 bytes x min(nnz, 2^26) + 32 bytes x nrows at any size. */
 int edx_pack_workspace(const edx_csr* A, size_t* bytes);
-/* Pass 1: *nnz_off, *nval, *vbits of complex128 square A.  EDX_ERR_OVERFLOW when A has too
- * many distinct off-diagonal values to pack.  Synchronises `stream`. */
-int edx_pack_count(const edx_csr* A, int64_t* nnz_off, int* nval, int* vbits, void* d_work,
+/* Pass 1: *nnz_off, *nval, *vbits (0 = wide) of complex128 square A, in the requested form
+ * (EDX_PACK_AUTO / _NARROW / _WIDE).  EDX_ERR_OVERFLOW when A has too many distinct
+ * off-diagonal values for that form.  Synchronises `stream`. */
+int edx_pack_count(const edx_csr* A, int form, int64_t* nnz_off, int* nval, int* vbits, void* d_work,
                    size_t work_bytes, void* stream);
-/* Pass 2: P->nnz, nval, vbits from pass 1 and its four arrays allocated by the caller;
- * d_work must still hold what pass 1 left in it. */
+/* Pass 2: P->nnz, nval, vbits from pass 1 and its arrays (vidx too for the wide form)
+ * allocated by the caller; d_work must still hold what pass 1 left in it. */
 int edx_pack_fill(const edx_csr* A, edx_packed* P, void* d_work, size_t work_bytes, void* stream);
+/* edx_spmm on the packed form: Y = alpha*(A X) + sigma*X + beta*Y over k complex128 columns
+ * (matvec_csr, src/spmv.f90:73-103, on the packed matrix).  The distinct values sit in
+ * shared memory; the diagonal term is added per row.  col_group as for edx_spmm. */
+int edx_spmm_packed(const edx_packed* P, int k, const double* d_x, int64_t ldx, double* d_y, int64_t ldy,
+                    double alpha_re, double alpha_im, double sigma_re, double sigma_im, double beta_re,
+                    double beta_im, int col_group, void* stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Block Gram-Schmidt for the ground-state eigensolver (the reorthogonalisation inside      */
@@ -281,6 +298,19 @@ typedef struct edx_krylov_opts {
      * one 32-bit word per off-diagonal entry and the value from a table in shared memory,
      * with the launch-shape fields above (the tiled layout takes precedence). */
     const edx_packed* apply_packed;
+    /* streaming projections, for problems where P_p V (every projected Lanczos vector) does
+     * not fit in memory.  With proj_window = B > 0, proj_out[p] holds only the last B
+     * projected vectors (device complex128[k][B][nrows_p]) and every B iterations (and at
+     * the end) they are folded into nacc accumulators:
+     *   acc_out[p][r * acc_ld + s] += sum_i acc_coef[s * maxn + i] * (P_p v_i)[column acc_col[s]][r]
+     * so that P_p (V y_s) is formed for coefficient vectors y_s (for example the per-shift
+     * MINRES coefficients of an earlier call with the same start vectors). */
+    int proj_window;
+    int nacc;
+    const int32_t* acc_col;      /* device int32[nacc]: Lanczos column of accumulator s */
+    const double* acc_coef;      /* device complex128[nacc * maxn] */
+    double* const* acc_out;      /* host array of nproj device pointers */
+    int64_t acc_ld;
 } edx_krylov_opts;
 
 /* k independent Lanczos recurrences of build_krylov_mp (src/lanczos.f90:210-303), run

@@ -124,8 +124,8 @@ def test_rixs_drop_in(cuda, golden_dir, workdir):
     assert rel_linf(s, s_ref) < 1e-6
 
 
-def test_rixs_batched_matches_reference_loop(cuda):
-    """All omega x pol_in x pol_out x gs from shared Krylov spaces == the per-point loop."""
+def _small_rixs():
+    """A 2-bath, N = 3 RIXS problem on the device and the oracle's per-point loop for it."""
     import torch
     from edrixs_b200 import device, rixs, siam
     m = siam.make_siam(2, 3, seed=4)
@@ -157,7 +157,34 @@ def test_rixs_batched_matches_reference_loop(cuda):
         Din=[device.build_csr(device.TRANS_I, bn, d, right=bi, num_val_orbs=nv, num_core_orbs=6) for d in din],
         Dout=[device.build_csr(device.TRANS_F, bi, d, right=bn, num_val_orbs=nv, num_core_orbs=6) for d in dout],
         gs_e=gs_e, gs_v=torch.from_numpy(gs_v).cuda())
+    return P, omegas, eloss, ref
+
+
+def test_rixs_batched_matches_reference_loop(cuda):
+    """All omega x pol_in x pol_out x gs from shared Krylov spaces == the per-point loop."""
+    from edrixs_b200 import rixs
+    P, omegas, eloss, ref = _small_rixs()
     res = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, nkryl=60, linsys_tol=1e-10, linsys_max=1000,
-                            temperature=300.0)
+                            temperature=300.0, stream=False)
     assert res.spectra.shape == ref.shape
     assert rel_linf(res.spectra, ref) < 1e-6
+
+
+@pytest.mark.parametrize("window", [1, 3, 8])
+def test_rixs_streamed_projections_match_stored(cuda, window):
+    """The two-pass form (shifted recurrences, then the same Lanczos vectors folded into the
+    final-state start vectors `window` at a time) equals the stored-projection form."""
+    import torch
+    from edrixs_b200 import rixs
+    P, omegas, eloss, ref = _small_rixs()
+    kw = dict(nkryl=60, linsys_tol=1e-10, linsys_max=1000, temperature=300.0)
+    a = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, stream=False, **kw)
+    b = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, stream=True, stream_window=window, **kw)
+    assert b.stats["streamed"] and not a.stats["streamed"]
+    assert np.array_equal(a.iters, b.iters)
+    assert torch.allclose(a.poles["norm"], b.poles["norm"], rtol=1e-12, atol=0)
+    n0 = int(a.poles["neff"].min().item())
+    assert torch.allclose(a.poles["alpha"][:, :min(n0, 10)], b.poles["alpha"][:, :min(n0, 10)], rtol=1e-10,
+                          atol=1e-10)
+    assert rel_linf(b.spectra, a.spectra) < 1e-8
+    assert rel_linf(b.spectra, ref) < 1e-6

@@ -45,12 +45,14 @@ def _assert_pack_lossless(P, A):
     assert np.array_equal(diag.view(np.float64), d.view(np.float64))
 
 
+@pytest.mark.parametrize("form", ["auto", "wide"])
 @pytest.mark.parametrize("mode", ["ham_i", "ham_n"])
-def test_pack_is_lossless(cuda, mode):
+def test_pack_is_lossless(cuda, mode, form):
     from edrixs_b200 import device
     ref, gpu = _ham(mode)
-    P = device.pack(gpu)
+    P = device.pack(gpu, form=form)
     assert P is not None and 0 < P.vals.numel() <= device.PACK_VALUES_MAX
+    assert P.wide == (form == "wide")
     _assert_pack_lossless(P, gpu)
 
 
@@ -133,3 +135,89 @@ def test_packed_krylov_shifts_and_projections(cuda):
     assert torch.equal(a.shift_iters, b.shift_iters)
     assert torch.allclose(a.shift_y, b.shift_y, rtol=1e-9, atol=1e-12)
     assert torch.allclose(a.proj[0], b.proj[0], rtol=1e-9, atol=1e-9)
+
+
+def _random_packable(n, per_row, nval, seed):
+    """n x n complex128 CSR with per_row distinct random columns per row (the diagonal among
+    them in some rows) and values drawn from nval distinct numbers."""
+    import torch
+    from edrixs_b200 import device
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    cols = torch.randint(0, n, (n, per_row), device="cuda", generator=g)
+    cols[::3, 0] = torch.arange(0, n, 3, device="cuda")  # a diagonal entry in every third row
+    cols, _ = torch.sort(cols, dim=1)
+    keep = torch.ones_like(cols, dtype=torch.bool)
+    keep[:, 1:] = cols[:, 1:] != cols[:, :-1]
+    counts = keep.sum(dim=1)
+    rp = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    rp[1:] = torch.cumsum(counts, 0)
+    col = cols[keep].to(torch.int32)
+    table = torch.complex(torch.randn(nval, device="cuda", dtype=torch.float64, generator=g),
+                          torch.randn(nval, device="cuda", dtype=torch.float64, generator=g))
+    val = table[torch.randint(0, nval, (col.numel(),), device="cuda", generator=g)]
+    return device.CSR(rp, col, val, n)
+
+
+def test_pack_wide_when_columns_leave_no_room(cuda):
+    """2^24 + 1 columns leave 7 bits of the 32-bit word: 300 distinct values need the wide
+    form.  "narrow" is refused, "auto" picks wide, and both products match the CSR's."""
+    import torch
+    from edrixs_b200 import device
+    A = _random_packable((1 << 24) + 1, 2, 300, seed=3)
+    assert device.pack(A, form="narrow") is None
+    P = device.pack(A)
+    assert P is not None and P.wide and P.vals.numel() == 300
+    _assert_pack_lossless(P, A)
+    rng = np.random.default_rng(1)
+    X = torch.from_numpy(rng.normal(size=(A.nrows, 3)) + 1j * rng.normal(size=(A.nrows, 3))).cuda()
+    ref = device.spmm(A, X)
+    got = device.spmm(P, X)
+    assert torch.allclose(got, ref, rtol=1e-12, atol=1e-12)
+
+
+def test_pack_count_in_chunks(cuda):
+    """More off-diagonal entries than one sort chunk (2^26): the count pass merges the chunks'
+    value tables."""
+    from edrixs_b200 import device
+    A = _random_packable(1_500_000, 48, 1000, seed=11)
+    assert A.nnz > (1 << 26) + 1_500_000
+    P = device.pack(A)  # 21 column bits leave 11 for the 1000 values: the narrow form
+    assert P is not None and not P.wide and P.vals.numel() == 1000
+    _assert_pack_lossless(P, A)
+
+
+@pytest.mark.parametrize("form", ["narrow", "wide"])
+@pytest.mark.parametrize("k", [1, 3, 6, 40])
+def test_spmm_packed_matches_csr(cuda, form, k):
+    import torch
+    from edrixs_b200 import device
+    ref, gpu = _ham("ham_n")
+    P = device.pack(gpu, form=form)
+    rng = np.random.default_rng(k)
+    X = torch.from_numpy(rng.normal(size=(gpu.nrows, k)) + 1j * rng.normal(size=(gpu.nrows, k))).cuda()
+    Y0 = torch.from_numpy(rng.normal(size=(gpu.nrows, k)) + 1j * rng.normal(size=(gpu.nrows, k))).cuda()
+    for al, sg, be in ((1.0, 0.0, 0.0), (-1.0, 2.5 + 0.5j, 0.0), (0.5j, 0.0, 1.0)):
+        a = device.spmm(gpu, X, Y0.clone(), alpha=al, sigma=sg, beta=be)
+        b = device.spmm(P, X, Y0.clone(), alpha=al, sigma=sg, beta=be)
+        assert torch.allclose(a, b, rtol=1e-12, atol=1e-12)
+    # against the oracle's y += A x for one column
+    x0 = X[:, 0].cpu().numpy()
+    assert np.allclose(device.spmm(P, X[:, 0].contiguous()).cpu().numpy(), orc.matvec(ref, x0), rtol=1e-12,
+                       atol=1e-12)
+
+
+@pytest.mark.parametrize("k", [6, 64])
+def test_wide_packed_krylov_matches_csr(cuda, k):
+    """Lanczos on the wide form, with the packed matrix passed in place of the CSR."""
+    import torch
+    from edrixs_b200 import device
+    ref, gpu = _ham("ham_n")
+    P = device.pack(gpu, form="wide")
+    rng = np.random.default_rng(k + 1)
+    V0 = torch.from_numpy(rng.normal(size=(gpu.nrows, k)) + 1j * rng.normal(size=(gpu.nrows, k))).cuda()
+    p = device.krylov(P, V0, 20)
+    c = device.krylov(gpu, V0, 20)
+    assert torch.equal(p.neff, c.neff)
+    assert torch.allclose(p.alpha, c.alpha, rtol=1e-10, atol=1e-10)
+    assert torch.allclose(p.beta, c.beta, rtol=1e-10, atol=1e-10)

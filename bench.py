@@ -125,7 +125,9 @@ def kernel_case_all(args):
     H_f, H_n, D_in and D_out, the one-column SpMV and the 6-column SpMM, two Lanczos steps
     on H_n (6 columns, with shifts and projections) and H_f (256 columns) on the CSR, packed
     and tiled forms with their builders, two MINRES steps on H_n, the continued fraction
-    (768 pole sets x 2000 points) and the density matrix."""
+    (768 pole sets x 2000 points), the density matrix, the packed SpMM (narrow and wide
+    forms), the Gram-Schmidt passes of the eigensolver and 16 Lanczos steps with streamed
+    projections."""
     import torch
     from edrixs_b200 import device
     m, t = workload_terms(args.nbath, args.nelec)
@@ -163,6 +165,21 @@ def kernel_case_all(args):
     device.cf_spectrum(torch.full((K,), nk, dtype=torch.int32, device="cuda"), al, be, np.zeros(K), np.ones(K),
                        np.ones(K), np.linspace(-0.5, 12.0, 2000), 0.1)
     device.denmat(bi, nv, crand(Hf.nrows, 3))
+    # products on the packed forms (narrow, and H_n in the wide form), the eigensolver's
+    # Gram-Schmidt passes, and the streamed projections of the two-pass RIXS
+    device.spmm(Pn, x1)
+    device.spmm(Pn, V[:, :3].contiguous())
+    Pw = device.pack(Hn, form="wide")
+    device.spmm(Pw, V[:, :3].contiguous())
+    device.krylov(Pw, V, 2, apply=dict(col_group=6, threads=1024, blocks_per_sm=1))
+    B = crand(45, Hn.nrows)
+    Wb = crand(Hn.nrows, 3)
+    C = device.gs_dot(B, 45, Wb)
+    device.gs_update(B, 45, Wb, C)
+    coef = crand(24, 16)
+    acc = torch.zeros((Dout.nrows, 24), dtype=torch.complex128, device="cuda")
+    device.krylov(Hn, seeds, 16, proj=[Dout], apply=dict(packed=Pn),
+                  accumulate=dict(window=8, col=shifts[0], coef=coef, out=[acc]))
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": "all", "nnz_Hn": Hn.nnz, "nnz_Hf": Hf.nnz, "nnz_Din": Din.nnz,
                       "nnz_Dout": Dout.nnz}))
@@ -856,7 +873,7 @@ def run_scale(args):
     P = rixs.RixsProblem(Hn=Pn, Hf=Pi, Din=[], Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v)
     P.packed.update(hn=Pn, hf=Pi)
     t0 = tick()
-    rc = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, seeds=seeds, final_block=64, **kw)
+    rc = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, seeds=seeds, final_block=128, **kw)
     tm["rixs_packed_s"] = tick() - t0
     npts = len(omegas) * 12
     res["rixs"] = {"omega_in": len(omegas), "points": npts, "minres_iters_max": int(rc.iters.max()),

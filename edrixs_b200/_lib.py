@@ -63,7 +63,7 @@ class KrylovOpts(ctypes.Structure):
                 ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int),
                 ("apply_layout", ctypes.POINTER(Tiles)), ("apply_packed", ctypes.POINTER(Packed)),
                 ("proj_window", ctypes.c_int), ("nacc", ctypes.c_int), ("acc_col", vp), ("acc_coef", vp),
-                ("acc_out", ctypes.POINTER(vp)), ("acc_ld", i64)]
+                ("acc_out", ctypes.POINTER(vp)), ("acc_ld", i64), ("v0_ld", i64)]
 
 
 _SIGS = {
@@ -99,6 +99,8 @@ _SIGS = {
     "edx_gs_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "edx_gs_dot": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp, ctypes.c_size_t, vp]),
     "edx_gs_update": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp]),
+    "edx_gs_gram": (ctypes.c_int, [vp, i64, ctypes.c_int, vp, vp, ctypes.c_size_t, vp]),
+    "edx_gs_rmul": (ctypes.c_int, [vp, i64, ctypes.c_int, vp, vp]),
     "edx_krylov_workspace": (ctypes.c_int, [i64, ctypes.c_int, ctypes.POINTER(KrylovOpts), ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_size_t)]),
     "edx_krylov": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.c_int, vp, ctypes.c_int, vp, vp, vp, vp,

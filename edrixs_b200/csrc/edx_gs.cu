@@ -41,13 +41,25 @@ __global__ void __launch_bounds__(GS_NT) k_gs_dot(int m, int64_t n, int64_t ldv,
 #pragma unroll
             for (int c = 0; c < K; ++c) acc[c] = make_double2(0.0, 0.0);
             const double2* vi = V + (int64_t)i * ldv + r0;
-            for (int rr = lane; rr < nr; rr += 32) {
-                const double2 v = __ldcs(vi + rr);
+            // four rows per lane per step: four loads in flight before the products
+            for (int rb = 0; rb < nr; rb += 128) {
+                double2 v[4];
 #pragma unroll
-                for (int c = 0; c < K; ++c) {
-                    const double2 p = conj_mul(v, wsm[rr * K + c]);
-                    acc[c].x += p.x;
-                    acc[c].y += p.y;
+                for (int q = 0; q < 4; ++q) {
+                    const int rr = rb + q * 32 + lane;
+                    v[q] = rr < nr ? __ldcs(vi + rr) : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int rr = rb + q * 32 + lane;
+                    if (rr < nr) {
+#pragma unroll
+                        for (int c = 0; c < K; ++c) {
+                            const double2 p = conj_mul(v[q], wsm[rr * K + c]);
+                            acc[c].x += p.x;
+                            acc[c].y += p.y;
+                        }
+                    }
                 }
             }
 #pragma unroll
@@ -114,6 +126,76 @@ __global__ void __launch_bounds__(GS_NT) k_gs_update(int m, int64_t n, int64_t l
     }
 }
 
+// part[block][a][c] = sum over this block's rows of conj(W[r, a]) W[r, c] (the k x k Gram
+// matrix of a row-major n x k block), then k_gs_sum; fixed row order per block
+template <int K>
+__global__ void __launch_bounds__(GS_NT) k_gs_gram(int64_t n, const double2* __restrict__ W,
+                                                    double2* __restrict__ part) {
+    __shared__ double2 red[GS_NW][K * K];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double2 acc[K * K];
+#pragma unroll
+    for (int e = 0; e < K * K; ++e) acc[e] = make_double2(0.0, 0.0);
+    for (int64_t r = (int64_t)blockIdx.x * GS_NT + threadIdx.x; r < n; r += (int64_t)gridDim.x * GS_NT) {
+        double2 w[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) w[c] = __ldcs(W + r * K + c);
+#pragma unroll
+        for (int a = 0; a < K; ++a)
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const double2 p = conj_mul(w[a], w[c]);
+                acc[a * K + c].x += p.x;
+                acc[a * K + c].y += p.y;
+            }
+    }
+#pragma unroll
+    for (int e = 0; e < K * K; ++e)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            acc[e].x += __shfl_xor_sync(0xffffffffu, acc[e].x, off);
+            acc[e].y += __shfl_xor_sync(0xffffffffu, acc[e].y, off);
+        }
+    if (lane == 0)
+#pragma unroll
+        for (int e = 0; e < K * K; ++e) red[warp][e] = acc[e];
+    __syncthreads();
+    for (int e = threadIdx.x; e < K * K; e += GS_NT) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int q = 0; q < GS_NW; ++q) {
+            s.x += red[q][e].x;
+            s.y += red[q][e].y;
+        }
+        part[(int64_t)blockIdx.x * K * K + e] = s;
+    }
+}
+
+// W = W M for a row-major n x k block and a k x k matrix M (row-major); a thread per row
+template <int K>
+__global__ void __launch_bounds__(GS_NT) k_gs_rmul(int64_t n, double2* __restrict__ W, const double2* __restrict__ M) {
+    __shared__ double2 msm[K * K];
+    for (int e = threadIdx.x; e < K * K; e += GS_NT) msm[e] = M[e];
+    __syncthreads();
+    for (int64_t r = (int64_t)blockIdx.x * GS_NT + threadIdx.x; r < n; r += (int64_t)gridDim.x * GS_NT) {
+        double2 w[K], o[K];
+#pragma unroll
+        for (int a = 0; a < K; ++a) {
+            w[a] = W[r * K + a];
+            o[a] = make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int a = 0; a < K; ++a)
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+                const double2 q = msm[a * K + c];
+                o[c].x += w[a].x * q.x - w[a].y * q.y;
+                o[c].y += w[a].x * q.y + w[a].y * q.x;
+            }
+#pragma unroll
+        for (int c = 0; c < K; ++c) W[r * K + c] = o[c];
+    }
+}
+
 int gs_blocks() { return num_sms() * 4; }
 
 template <template <int> class F, class... A>
@@ -174,6 +256,30 @@ struct UpdRun {
     }
 };
 
+template <int K>
+struct GramRun {
+    static int run(int64_t n, const double2* W, double2* part, double2* G, cudaStream_t st) {
+        const int nb = gs_blocks();
+        k_gs_gram<K><<<nb, GS_NT, 0, st>>>(n, W, part);
+        EDX_CHECK_LAUNCH();
+        const int me = K * K;
+        k_gs_sum<<<(me * 32 + 255) / 256, 256, 0, st>>>(nb, me, part, G);
+        EDX_CHECK_LAUNCH();
+        return EDX_OK;
+    }
+};
+
+template <int K>
+struct RmulRun {
+    static int run(int64_t n, double2* W, const double2* M, cudaStream_t st) {
+        const int64_t need = (n + GS_NT - 1) / GS_NT;
+        const int nb = (int)std::min<int64_t>(need, (int64_t)num_sms() * 8);
+        k_gs_rmul<K><<<nb, GS_NT, 0, st>>>(n, W, M);
+        EDX_CHECK_LAUNCH();
+        return EDX_OK;
+    }
+};
+
 int check_gs(int m, int64_t n, int64_t ldv, int k, const void* V, const void* W, const void* C) {
     EDX_REQUIRE(V && W && C, "edx_gs: NULL pointer");
     EDX_REQUIRE(m >= 1 && n >= 1 && ldv >= n && k >= 1 && k <= GS_KMAX, "edx_gs: bad sizes");
@@ -214,4 +320,20 @@ extern "C" int edx_gs_update(const double* d_V, int m, int64_t n, int64_t ldv, d
     if (rc) return rc;
     return dispatch_k<UpdRun>(k, m, n, ldv, reinterpret_cast<const double2*>(d_V), reinterpret_cast<double2*>(d_W),
                               reinterpret_cast<const double2*>(d_C), as_stream(stream));
+}
+
+extern "C" int edx_gs_gram(const double* d_W, int64_t n, int k, double* d_G, void* d_work, size_t work_bytes,
+                           void* stream) {
+    EDX_REQUIRE(d_W && d_G && n >= 1 && k >= 1 && k <= GS_KMAX, "edx_gs_gram: bad arguments");
+    Workspace w(d_work, work_bytes);
+    double2* part = w.take<double2>((size_t)gs_blocks() * k * k);
+    if (!part) return fail(EDX_ERR_WORKSPACE, "edx_gs_gram: workspace too small");
+    return dispatch_k<GramRun>(k, n, reinterpret_cast<const double2*>(d_W), part, reinterpret_cast<double2*>(d_G),
+                               as_stream(stream));
+}
+
+extern "C" int edx_gs_rmul(double* d_W, int64_t n, int k, const double* d_M, void* stream) {
+    EDX_REQUIRE(d_W && d_M && n >= 1 && k >= 1 && k <= GS_KMAX, "edx_gs_rmul: bad arguments");
+    return dispatch_k<RmulRun>(k, n, reinterpret_cast<double2*>(d_W), reinterpret_cast<const double2*>(d_M),
+                               as_stream(stream));
 }

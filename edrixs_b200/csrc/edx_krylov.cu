@@ -544,14 +544,15 @@ __global__ void k_proj_accum(int64_t m, int B, int nb, int i0, int64_t maxn, int
 
 // ---- start vectors: norm and normalisation --------------------------------------------
 template <int KW>
-__global__ void __launch_bounds__(KT) k_colnorm(int64_t n, const double2* __restrict__ V0, KrylovState S) {
+__global__ void __launch_bounds__(KT) k_colnorm(int64_t n, const double2* __restrict__ V0, int64_t ld0,
+                                                KrylovState S) {
     const int k = S.k;
     const int c = threadIdx.x % KW, g = threadIdx.x / KW, groups = KT / KW;
     const int gc = blockIdx.y * KW + c;
     double part = 0.0;
     if (gc < k)
         for (int64_t r = (int64_t)blockIdx.x * groups + g; r < n; r += (int64_t)gridDim.x * groups) {
-            double2 v = V0[r * k + gc];
+            double2 v = V0[r * ld0 + gc];
             part += v.x * v.x + v.y * v.y;
         }
     block_col_partial<KW>(part, true, g, groups, c, k, S.part);
@@ -569,13 +570,14 @@ __global__ void __launch_bounds__(KT) k_colnorm(int64_t n, const double2* __rest
     }
 }
 
-__global__ void k_start(int64_t n, int k, const double2* __restrict__ V0, double2* __restrict__ Vc,
+__global__ void k_start(int64_t n, int k, const double2* __restrict__ V0, int64_t ld0, double2* __restrict__ Vc,
                         double2* __restrict__ Vp, const double* __restrict__ s) {
     const int64_t total = n * k;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
          e += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(e % k);
-        double2 v = V0[e];
+        const int64_t r = e / k;
+        const int c = (int)(e - r * k);
+        double2 v = V0[r * ld0 + c];
         const double d = s[c];
         Vc[e] = make_double2(v.x / d, v.y / d);
         Vp[e] = make_double2(0.0, 0.0);
@@ -899,6 +901,8 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
                 "edx_krylov: bad arguments");
     const int nshift = opts ? opts->nshift : 0;
     const int nproj = opts ? opts->nproj : 0;
+    const int64_t ld0 = (opts && opts->v0_ld > 0) ? opts->v0_ld : k;
+    EDX_REQUIRE(ld0 >= k, "edx_krylov: v0_ld must be >= k");
     if (nshift > 0)
         EDX_REQUIRE(opts->shift_col && opts->shift_z && opts->shift_y, "edx_krylov: shift arrays missing");
     for (int p = 0; p < nproj; ++p) {
@@ -980,12 +984,12 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     const double2* V0 = reinterpret_cast<const double2*>(d_v0);
     {
         dim3 grid(reduce_grid(n), gy);
-        EDX_KW_SWITCH(kw, k_colnorm, grid, n, V0, S);
+        EDX_KW_SWITCH(kw, k_colnorm, grid, n, V0, ld0, S);
         EDX_CHECK_LAUNCH();
     }
     EDX_CUDA(cudaMemcpyAsync(d_norm, ws.alpha, sizeof(double) * k, cudaMemcpyDeviceToDevice, st));
     const int eb = (int)std::min<int64_t>((n * k + 255) / 256, (int64_t)num_sms() * 16);
-    k_start<<<eb, 256, 0, st>>>(n, k, V0, ws.Vc, ws.Vp, ws.beta);
+    k_start<<<eb, 256, 0, st>>>(n, k, V0, ld0, ws.Vc, ws.Vp, ws.beta);
     EDX_CHECK_LAUNCH();
     if (nshift > 0) {
         EDX_CUDA(cudaMemsetAsync(ws.wbuf, 0, sizeof(double2) * 2 * (size_t)nshift * maxn, st));

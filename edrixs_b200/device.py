@@ -423,7 +423,9 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
         apply = dict(apply or {}, packed=A)
         if apply.get("layout") is not None:
             raise ValueError("krylov: a packed matrix has no tiled layout")
-    V0 = V0.reshape(V0.shape[0], -1).contiguous()
+    V0 = V0.reshape(V0.shape[0], -1)
+    if (V0.shape[1] > 1 and V0.stride(1) != 1) or V0.stride(0) < V0.shape[1]:
+        V0 = V0.contiguous()
     n, k = V0.shape
     dev = V0.device
     alpha = torch.zeros((k, maxn), dtype=torch.float64, device=dev)
@@ -431,6 +433,7 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
     norm = torch.zeros(k, dtype=torch.float64, device=dev)
     neff = torch.zeros(k, dtype=torch.int32, device=dev)
     opts = KrylovOpts()
+    opts.v0_ld = V0.stride(0)  # the start vectors may be columns of a wider row-major block
     keep = []
     outs = []
     if proj:
@@ -540,6 +543,27 @@ def gs_dot(V, m, W):
     w = _work(ws.value)
     call("edx_gs_dot", _ptr(V), m, n, V.stride(0), _ptr(W), k, _ptr(C), _ptr(w), ws.value, _stream())
     return C
+
+
+def gs_gram(W):
+    """G = W^H W (k x k) for a row-major (n, k) block, k <= 8."""
+    n, k = W.shape
+    assert W.is_contiguous()
+    G = torch.empty((k, k), dtype=torch.complex128, device=W.device)
+    ws = ctypes.c_size_t(0)
+    call("edx_gs_workspace", k, k, ctypes.byref(ws))
+    w = _work(ws.value)
+    call("edx_gs_gram", _ptr(W), n, k, _ptr(G), _ptr(w), ws.value, _stream())
+    return G
+
+
+def gs_rmul(W, M):
+    """W = W M in place for a row-major (n, k) block and a (k, k) matrix."""
+    n, k = W.shape
+    assert W.is_contiguous()
+    Mc = torch.as_tensor(M, dtype=torch.complex128).to(W.device).contiguous()
+    call("edx_gs_rmul", _ptr(W), n, k, _ptr(Mc), _stream())
+    return W
 
 
 def gs_update(V, m, W, C):

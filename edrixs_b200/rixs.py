@@ -189,7 +189,7 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     hf_ms, hf_it = 0.0, 0
     for s in range(0, K, blk):
         e = min(K, s + blk)
-        rf = device.krylov(P.Hf, V0[:, s:e].contiguous(), nkryl, c64=c64_f, timing=timing, apply=cfg_hf)
+        rf = device.krylov(P.Hf, V0[:, s:e], nkryl, c64=c64_f, timing=timing, apply=cfg_hf)
         A[s:e], B[s:e], NRM[s:e], NEFF[s:e] = rf.alpha, rf.beta, rf.norm, rf.neff
         hf_ms += rf.apply_ms or 0.0
         hf_it += rf.apply_launches

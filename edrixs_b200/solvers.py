@@ -29,17 +29,23 @@ def _qr(W):
     return Q, R
 
 
-def _cholqr2(W):
+def _cholqr2(W, gram=None, rmul=None):
     """W = Q R for a tall-skinny block by CholeskyQR2 (Fukaya, Nakatsukasa, Yanagisawa,
     Yamamoto 2014): twice, R from the Cholesky factor of the small Gram matrix W^H W and
     Q = W R^-1.  Two passes over W instead of a Householder factorisation, which is slow for
     millions of rows and a few columns.  A block too ill-conditioned for it (a Krylov space
-    about to break down) goes to Householder QR."""
+    about to break down) goes to Householder QR.  gram(Q) -> Q^H Q and rmul(Q, M): Q = Q M in
+    place; libedx's single-pass kernels (edx_gs_gram / edx_gs_rmul) unless given.  Returns
+    (Q, R) with R a host array (a device tensor on the Householder path)."""
+    gram = gram or device.gs_gram
+    rmul = rmul or device.gs_rmul
     k = W.shape[1]
-    Q = W
+    if k > 8:
+        return _qr(W)
+    Q = W.contiguous().clone()
     Rt = np.eye(k, dtype=np.complex128)
     for _ in range(2):
-        G = (Q.conj().T @ Q).cpu().numpy()
+        G = gram(Q).cpu().numpy()
         G = 0.5 * (G + G.conj().T)
         try:
             L = np.linalg.cholesky(G)
@@ -49,9 +55,9 @@ def _cholqr2(W):
         d = np.abs(np.diag(R))
         if not np.all(np.isfinite(d)) or d.min() <= 1e-7 * d.max():
             return _qr(W)
-        Q = Q @ torch.from_numpy(np.linalg.inv(R)).to(W.device)
+        rmul(Q, np.linalg.inv(R))   # Q = Q R^-1 in place
         Rt = R @ Rt
-    return Q.contiguous(), torch.from_numpy(Rt).to(W.device)
+    return Q, Rt
 
 
 def dense_eigs(H: device.CSR, nev):
@@ -107,7 +113,7 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
             Q, R = _cholqr2(W)
             V[j + b:j + 2 * b] = Q.T
             T[:j + b, j:j + b] = C.cpu().numpy()
-            T[j + b:j + 2 * b, j:j + b] = R.cpu().numpy()
+            T[j + b:j + 2 * b, j:j + b] = R if isinstance(R, np.ndarray) else R.cpu().numpy()
             j += b
         m = mmax
         Tm = T[:m, :m]

@@ -43,9 +43,10 @@ def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None,
     key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64), layout is not None, packed is not None)
     if key in _cache:
         return _cache[key]
-    g = torch.Generator(device=A.val.device)
+    dev = A.row_ptr.device
+    g = torch.Generator(device=dev)
     g.manual_seed(1)
-    V0 = torch.randn((A.nrows, k), dtype=torch.float64, device=A.val.device, generator=g).to(torch.complex128)
+    V0 = torch.randn((A.nrows, k), dtype=torch.float64, device=dev, generator=g).to(torch.complex128)
     best, best_t = None, float("inf")
     results = []
     cands = candidates(k)

@@ -244,6 +244,12 @@ int edx_gs_dot(const double* d_V, int m, int64_t n, int64_t ldv, const double* d
                void* d_work, size_t work_bytes, void* stream);
 int edx_gs_update(const double* d_V, int m, int64_t n, int64_t ldv, double* d_W, int k, const double* d_C,
                   void* stream);
+/* The two passes of CholeskyQR for the block W (n x k row-major, k <= 8):
+ * edx_gs_gram: G = W^H W (k x k row-major; deterministic as edx_gs_dot; workspace from
+ *              edx_gs_workspace(k, k, ...))
+ * edx_gs_rmul: W = W M for a k x k row-major M (e.g. the inverse Cholesky factor). */
+int edx_gs_gram(const double* d_W, int64_t n, int k, double* d_G, void* d_work, size_t work_bytes, void* stream);
+int edx_gs_rmul(double* d_W, int64_t n, int k, const double* d_M, void* stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Lanczos / Krylov                                                                     */
@@ -311,11 +317,14 @@ typedef struct edx_krylov_opts {
     const double* acc_coef;      /* device complex128[nacc * maxn] */
     double* const* acc_out;      /* host array of nproj device pointers */
     int64_t acc_ld;
+    /* leading dimension of d_v0 (0 = k): the start vectors may be k columns of a wider
+     * row-major block */
+    int64_t v0_ld;
 } edx_krylov_opts;
 
 /* k independent Lanczos recurrences of build_krylov_mp (src/lanczos.f90:210-303), run
  * together so that every iteration is one SpMM over k columns (FP64 recurrence).  d_v0:
- * n x k (ld = k) start vectors.  Outputs for column j: d_alpha[j*maxn + i],
+ * n x k start vectors, row-major with leading dimension opts->v0_ld (k when 0).  Outputs for column j: d_alpha[j*maxn + i],
  * d_beta[j*maxn + i] (i < neff), d_norm[j] = <v0_j|v0_j>, d_neff[j].  Column j stops when
  * beta < 1e-10 (absolute, :291).  The matrix may be complex128 or complex64 (vectors and
  * scalars stay complex128 / FP64). */

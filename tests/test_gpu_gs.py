@@ -29,3 +29,36 @@ def test_gs_dot_update(cuda, m, n, k):
     device.gs_update(Vfull, m, W2, C)
     want2 = W - Vfull[:m].T @ C
     assert torch.allclose(W2, want2, rtol=1e-12, atol=1e-12 * want2.abs().max().item())
+
+
+@pytest.mark.parametrize("n,k", [(7, 1), (70001, 3), (5000, 8)])
+def test_gs_gram_rmul(cuda, n, k):
+    """edx_gs_gram == W^H W and edx_gs_rmul == W M (1e-12 relative), gram deterministic."""
+    import torch
+    from edrixs_b200 import device
+    g = torch.Generator(device="cuda")
+    g.manual_seed(n + k)
+    W = torch.complex(torch.randn((n, k), dtype=torch.float64, device="cuda", generator=g),
+                      torch.randn((n, k), dtype=torch.float64, device="cuda", generator=g))
+    G = device.gs_gram(W)
+    want = W.conj().T @ W
+    assert torch.allclose(G, want, rtol=1e-12, atol=1e-12 * want.abs().max().item())
+    assert torch.equal(G, device.gs_gram(W))
+    M = torch.complex(torch.randn((k, k), dtype=torch.float64, device="cuda", generator=g),
+                      torch.randn((k, k), dtype=torch.float64, device="cuda", generator=g))
+    want2 = W @ M
+    device.gs_rmul(W, M)
+    assert torch.allclose(W, want2, rtol=1e-12, atol=1e-12 * want2.abs().max().item())
+
+
+def test_cholqr2_on_device(cuda):
+    import torch
+    from edrixs_b200 import solvers
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    W = torch.complex(torch.randn((200_000, 3), dtype=torch.float64, device="cuda", generator=g),
+                      torch.randn((200_000, 3), dtype=torch.float64, device="cuda", generator=g))
+    Q, R = solvers._cholqr2(W)
+    R = torch.as_tensor(R).to(W.device)
+    assert torch.allclose(Q.conj().T @ Q, torch.eye(3, dtype=torch.complex128, device="cuda"), atol=1e-13)
+    assert torch.allclose(Q @ R, W, atol=1e-10)

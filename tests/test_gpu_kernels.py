@@ -208,6 +208,20 @@ def test_krylov_matches_oracle(hn_pair):
         assert np.allclose(res.beta[c].cpu().numpy()[:neff], b, rtol=1e-8, atol=1e-8)
 
 
+def test_krylov_start_columns_of_a_wider_block(hn_pair):
+    """Start vectors given as a column slice of a wider row-major block (leading dimension >
+    k) give the same recurrences as the same columns copied out."""
+    import torch
+    from edrixs_b200 import device
+    ref, gpu = hn_pair
+    rng = np.random.default_rng(2)
+    W = torch.from_numpy(rng.normal(size=(gpu.nrows, 7)) + 1j * rng.normal(size=(gpu.nrows, 7))).cuda()
+    for s, e in ((2, 5), (6, 7)):
+        a = device.krylov(gpu, W[:, s:e], 20)
+        b = device.krylov(gpu, W[:, s:e].contiguous(), 20)
+        assert torch.equal(a.alpha, b.alpha) and torch.equal(a.beta, b.beta) and torch.equal(a.norm, b.norm)
+
+
 def test_krylov_early_stop(cuda, golden_dir):
     """A 45-dimensional space exhausts before maxn: beta < 1e-10 stops the column (:291)."""
     import torch

@@ -747,8 +747,10 @@ def run_scale(args):
     import gc
     import math
     import torch
-    from edrixs_b200 import device, rixs, solvers
+    from edrixs_b200 import device, rixs, solvers, tune
     nb, N = args.scale_nbath, args.scale_nelec
+    # final-state block launch shape (the one the autotuner picks for H_f at 768 columns)
+    hf_cfg = dict(col_group=32, tiles=2, threads=256, blocks_per_sm=4, chunked=0, packed=1)
     m, t = workload_terms(nb, N)
     nv = m.nv
     res = {"config": {"workload": f"XAS + RIXS at scale: 10 impurity + {nb} bath spin-orbitals, N={N}",
@@ -798,12 +800,16 @@ def run_scale(args):
     res["H_n"] = {"nnz": Hn.nnz, "csr_c128_gb": gb(Hn.nbytes()), "csr_c64_gb": gb(Hn.nbytes(c64=True))}
     nk = 200
 
-    def xas(A, c64=False):
+    def xas(A, c64=False, cfg=None):
         ta = tick()
-        kr = device.krylov(A, seeds, nk, c64=c64, timing=True)
+        kr = device.krylov(A, seeds, nk, c64=c64, timing=True, apply=cfg)
         return kr, tick() - ta
 
-    xa, tm["xas_fp64_csr_s"] = xas(Hn)
+    t0 = tick()
+    cfg_csr = tune.tune_apply(Hn, seeds.shape[1])
+    tm["tune_hn_csr_s"] = tick() - t0
+    res["H_n"]["csr_launch_shape"] = cfg_csr
+    xa, tm["xas_fp64_csr_s"] = xas(Hn, cfg=cfg_csr)
     tm["xas_fp64_csr_apply_ms_per_step"] = xa.apply_ms / max(xa.apply_launches, 1)
     # edge from the lowest Ritz value of the XAS recurrence of the ground state
     ne = int(xa.neff[0].item())
@@ -828,7 +834,9 @@ def run_scale(args):
     Hn = device.build_csr(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6,
                           values="c64")
     tm["hn_build_c64_s"] = tick() - t0
-    xb, tm["xas_c64_csr_s"] = xas(Hn, c64=True)
+    cfg_c64 = tune.tune_apply(Hn, seeds.shape[1], c64=True)
+    res["H_n"]["c64_launch_shape"] = cfg_c64
+    xb, tm["xas_c64_csr_s"] = xas(Hn, c64=True, cfg=cfg_c64)
     tm["xas_c64_csr_apply_ms_per_step"] = xb.apply_ms / max(xb.apply_launches, 1)
     sb = xas_spec(xb)
     res["xas"] = {"steps": nk, "columns": seeds.shape[1], "grid_points": len(grid), "gamma": 0.3,
@@ -843,6 +851,8 @@ def run_scale(args):
     kw = dict(nkryl=150, linsys_tol=1e-10, linsys_max=1000, temperature=300.0, stream=True, timing=True)
     P = rixs.RixsProblem(Hn=Hn, Hf=Pi, Din=[], Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v)
     P.packed["hf"] = Pi
+    P.meta[("apply", "hn", seeds.shape[1], True)] = cfg_c64
+    P.meta[("apply", "hf", 128, False)] = hf_cfg
     t0 = tick()
     rb = rixs.rixs_spectra(P, omegas[sub], 0.6, eloss, 0.1, c64=True, c64_final=False, seeds=seeds,
                            final_block=128, **kw)
@@ -866,12 +876,18 @@ def run_scale(args):
     tm.update(hn_rebuild_s=t1 - t0, hn_pack_s=t2 - t1, hi_dout_rebuild_s=tick() - t2)
     res["H_n"].update(packed_gb=gb(Pn.nbytes()), packed_form="wide" if Pn.wide else "narrow",
                       distinct_values=Pn.vals.numel())
-    xc, tm["xas_packed_s"] = xas(Pn)
+    t0 = tick()
+    cfg_pk = tune.tune_apply(Pn, seeds.shape[1])
+    tm["tune_hn_packed_s"] = tick() - t0
+    res["H_n"]["packed_launch_shape"] = cfg_pk
+    xc, tm["xas_packed_s"] = xas(Pn, cfg=cfg_pk)
     tm["xas_packed_apply_ms_per_step"] = xc.apply_ms / max(xc.apply_launches, 1)
     res["xas"]["packed_vs_fp64_rel_linf"] = rel(xas_spec(xc), sa)
     del xc
     P = rixs.RixsProblem(Hn=Pn, Hf=Pi, Din=[], Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v)
     P.packed.update(hn=Pn, hf=Pi)
+    P.meta[("apply", "hn", seeds.shape[1], False)] = cfg_pk
+    P.meta[("apply", "hf", 128, False)] = hf_cfg
     t0 = tick()
     rc = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, seeds=seeds, final_block=128, **kw)
     tm["rixs_packed_s"] = tick() - t0

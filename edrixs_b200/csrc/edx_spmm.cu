@@ -232,17 +232,17 @@ __global__ void __launch_bounds__(256) k_spmm_packed(int64_t nrows, PackedView M
         }
         *yp = make_double2(yr, yi);
     };
-    if (KW == 1) {  // one column: the next row's words load during this row
+    if constexpr (KW == 1) {  // one column: the next row's words load during this row
         spmv_rows_packed<WIDE>(warp0, nrows, nw, M, sp_tab, X, ldx_, col0, [&](int64_t r, double2 acc) {
             if (lane == 0) store(r, acc);
         });
-        return;
-    }
-    for (int64_t r = warp0; r < nrows; r += nw) {
-        const int64_t s = __ldg(M.row_ptr + r), e = __ldg(M.row_ptr + r + 1);
-        double2 acc[1];
-        row_times_x_packed<KW, 1, WIDE>(s, e, M.ent, M.vidx, M.vbits, sp_tab, X, ldx_, col0, k, acc);
-        if (lane < KW && gc < k) store(r, acc[0]);
+    } else {
+        for (int64_t r = warp0; r < nrows; r += nw) {
+            const int64_t s = __ldg(M.row_ptr + r), e = __ldg(M.row_ptr + r + 1);
+            double2 acc[1];
+            row_times_x_packed<KW, 1, WIDE>(s, e, M.ent, M.vidx, M.vbits, sp_tab, X, ldx_, col0, k, acc);
+            if (lane < KW && gc < k) store(r, acc[0]);
+        }
     }
 }
 

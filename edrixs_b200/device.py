@@ -403,7 +403,7 @@ class KrylovResult:
     beta: torch.Tensor    # (k, maxn)
     norm: torch.Tensor    # (k,)
     neff: torch.Tensor    # (k,) int32
-    proj: list            # per projector: (k, maxn, nrows_p) complex128
+    proj: list            # per projector: (k, steps + 1 (<= maxn), nrows_p) complex128
     shift_y: Optional[torch.Tensor] = None      # (nshift, maxn) complex128
     shift_iters: Optional[torch.Tensor] = None
     shift_res: Optional[torch.Tensor] = None
@@ -439,7 +439,8 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
     if proj:
         depth = int(accumulate["window"]) if accumulate else maxn
         descs = (Csr * len(proj))(*[P.desc() for P in proj])
-        outs = [torch.zeros((k, depth, P.nrows), dtype=torch.complex128, device=dev) for P in proj]
+        # every slot that is returned gets written: no clearing pass over what can be tens of GB
+        outs = [torch.empty((k, depth, P.nrows), dtype=torch.complex128, device=dev) for P in proj]
         ptrs = (ctypes.c_void_p * len(proj))(*[o.data_ptr() for o in outs])
         opts.nproj = len(proj)
         opts.proj = descs
@@ -511,7 +512,9 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
     adesc = A.shape_desc() if isinstance(A, PackedMatrix) else A.desc(c64)
     call("edx_krylov", ctypes.byref(adesc), k, _ptr(V0), maxn, _ptr(alpha), _ptr(beta), _ptr(norm),
          _ptr(neff), ctypes.byref(opts), _ptr(w), ws.value, _stream())
-    res = KrylovResult(alpha, beta, norm, neff, [] if accumulate else outs, sy, si, sr)
+    # projected vectors exist for v_0 .. v_L after L iterations
+    written = min(nl.value + 1, maxn)
+    res = KrylovResult(alpha, beta, norm, neff, [] if accumulate else [o[:, :written, :] for o in outs], sy, si, sr)
     res.apply_ms = ms.value if timing else None
     res.apply_launches = nl.value
     return res

@@ -22,7 +22,7 @@ Here:
     the Boltzmann sum over ground states (edrixs/utils.py:54-73).
 """
 from dataclasses import dataclass, field
-from typing import List
+from typing import List, Optional
 
 import numpy as np
 import torch
@@ -86,6 +86,8 @@ class RixsResult:
     res: np.ndarray          # |res| estimates
     krylov_steps: int        # Lanczos steps taken on H_n
     stats: dict = field(default_factory=dict)  # kernel launch counts and timings
+    spectra_gs: Optional[np.ndarray] = None  # per ground state, before the Boltzmann sum:
+    #                                          (n_omega, n_eloss, n_pol_in * n_pol_out, ngs)
 
 
 def _stream_needed(P, k, maxn):
@@ -98,13 +100,14 @@ def _stream_needed(P, k, maxn):
 
 def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, linsys_tol=1e-10,
                  linsys_max=1000, temperature=300.0, c64=False, final_block=None, timing=False, autotune=False,
-                 stream=None, stream_window=8, seeds=None, c64_final=None):
+                 stream=None, stream_window=8, seeds=None, c64_final=None, per_gs=False):
     """RIXS spectra of every (omega_in, pol_in, pol_out, gs) of one request.
     stream: None (automatic), True or False -- whether D_out^+ v_i is folded into the
     final-state start vectors as the Lanczos vectors appear (two passes over H_n) instead of
     being stored for every v_i.  seeds: the block D_in(pol_in)|g> (n_n, npin * ngs), column
     p_in * ngs + g, when the caller computed it already (P.Din is then not used).  c64: the
-    H_n products (MINRES part) in complex64; c64_final: the H_f products too (default: as c64)."""
+    H_n products (MINRES part) in complex64; c64_final: the H_f products too (default: as c64).
+    per_gs: also return the spectra of each ground state before the Boltzmann sum."""
     c64_f = c64 if c64_final is None else bool(c64_final)
     omegas = np.asarray(omegas, dtype=np.float64)
     eloss = np.asarray(eloss, dtype=np.float64)
@@ -207,8 +210,9 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     w = torch.from_numpy(boltz(P.gs_e, temperature)).to(dev)
     out = torch.einsum("oigwe,g->weio", spec, w).reshape(n_om, ne, npin * npout)
     stats["launches"] += 1
+    per_g = spec.permute(3, 4, 1, 0, 2).reshape(n_om, ne, npin * npout, ngs).cpu().numpy() if per_gs else None
     return RixsResult(out.cpu().numpy(), dict(alpha=A, beta=B, norm=NRM, neff=NEFF, e0=e0), iters, resid, steps,
-                      stats)
+                      stats, per_g)
 
 
 def rixs_request(P: RixsProblem, gs_v_host, omegas, gamma_c, eloss, gamma_f, **kw):

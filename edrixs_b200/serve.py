@@ -166,6 +166,21 @@ def estimate_bytes(req: Request, resident_cached: bool):
     return int(resident + work)
 
 
+def coalesce_key(req: Request):
+    """Requests with equal keys share one solve: RIXS on one Hamiltonian with the same
+    linewidths, Lanczos and MINRES settings, temperature and loss grid (their incident
+    energies, polarisations and ground-state counts may differ: the solve takes the union and
+    the largest count, and each request gets its own columns and Boltzmann sum back); XAS on
+    one Hamiltonian with the same Lanczos length (one Krylov launch over all their start
+    vectors).  ED requests are not coalesced."""
+    if req.kind == "rixs":
+        return ("rixs", req.model, req.gamma_c, req.gamma_f, req.nkryl, req.linsys_tol, req.linsys_max,
+                req.temperature, len(req.eloss), float(req.eloss[0]), float(req.eloss[-1]))
+    if req.kind == "xas":
+        return ("xas", req.model, req.nkryl)
+    return None
+
+
 class Server:
     def __init__(self, hbm_budget=150e9, workers=2):
         self.budget = float(hbm_budget)
@@ -178,6 +193,9 @@ class Server:
         self.stop_flag = False
         self.records = []
         self.threads = []
+        # a request is taken from the waiting list only when a worker is free, so that the
+        # requests which arrive meanwhile can join its solve (coalesce_key)
+        self.free_workers = workers
 
     # -- public ---------------------------------------------------------------------------
     def start(self):
@@ -237,6 +255,9 @@ class Server:
             with self.cv:
                 if self.stop_flag:
                     return
+                if self.free_workers == 0 or not self.waiting:
+                    self.cv.wait(timeout=0.05)
+                    continue
                 picked = None
                 for i, (req, fut) in enumerate(self.waiting):
                     cached = req.model in self.residents
@@ -251,23 +272,17 @@ class Server:
                     continue
                 req, fut = self.waiting.pop(picked)
                 group = [(req, fut)]
-                if req.kind == "rixs":  # coalesce waiting RIXS on the same Hamiltonian and settings
-                    sig = (req.model, req.ngs, req.gamma_c, req.gamma_f, tuple(req.pols), req.nkryl, req.linsys_tol,
-                           req.linsys_max, req.temperature, len(req.eloss), float(req.eloss[0]), float(req.eloss[-1]))
+                sig = coalesce_key(req)
+                if sig is not None:  # waiting requests that can share this one's solve
                     rest = []
                     for r2, f2 in self.waiting:
-                        s2 = (r2.model, r2.ngs, r2.gamma_c, r2.gamma_f, tuple(r2.pols), r2.nkryl, r2.linsys_tol,
-                              r2.linsys_max, r2.temperature, len(r2.eloss), float(r2.eloss[0]),
-                              float(r2.eloss[-1])) if r2.kind == "rixs" else None
-                        if s2 == sig:
-                            group.append((r2, f2))
-                        else:
-                            rest.append((r2, f2))
+                        (group if coalesce_key(r2) == sig else rest).append((r2, f2))
                     self.waiting = rest
                 need = sum(estimate_bytes(r, r.model in self.residents) for r, _ in group)
                 res = self._resident(req.model)
                 res.busy += 1
                 self.inflight_bytes += need
+                self.free_workers -= 1
             self.jobs.put((group, res, need))
 
     def _work(self, idx):
@@ -296,6 +311,7 @@ class Server:
                 with self.cv:
                     res.busy -= 1
                     self.inflight_bytes -= need
+                    self.free_workers += 1
                     self.cv.notify_all()
 
     # -- solves ---------------------------------------------------------------------------
@@ -304,39 +320,54 @@ class Server:
         if req.kind == "ed":
             res.ensure(False, req.ngs)
             return [{"eigvals": res.gs_e[:r.ngs].copy()} for r, _ in group]
-        res.ensure(True, req.ngs)
+        G = max(r.ngs for r, _ in group)
+        res.ensure(True, G)
         if req.kind == "xas":
-            return [self._xas(r, res) for r, _ in group]
-        # union of incident energies (absolute) over the coalesced requests
+            return self._xas_group(group, res)
+        # union of incident energies (absolute) and polarisations over the coalesced requests
         oms = [np.asarray(r.omegas, dtype=np.float64) + res.edge for r, _ in group]
         allw = np.unique(np.concatenate(oms))
-        pins = sorted(set(siam_pol_in(p) for p in req.pols))
-        pouts = sorted(set(siam_pol_out(p) for p in req.pols))
+        pins = sorted(set(siam_pol_in(p) for r, _ in group for p in r.pols))
+        pouts = sorted(set(siam_pol_out(p) for r, _ in group for p in r.pols))
         P = rixs.RixsProblem(Hn=res.Hn, Hf=res.Hi, Din=[res.op("in", p) for p in pins],
-                             Dout=[res.op("out", p) for p in pouts], gs_e=res.gs_e[:req.ngs],
-                             gs_v=res.gs_v[:, :req.ngs].contiguous(),
+                             Dout=[res.op("out", p) for p in pouts], gs_e=res.gs_e[:G],
+                             gs_v=res.gs_v[:, :G].contiguous(),
                              packed={k: v for k, v in (("hf", res.packed.get("hi")), ("hn", res.packed.get("hn")))
                                      if v is not None})
         out = rixs.rixs_spectra(P, allw, req.gamma_c, req.eloss, req.gamma_f, nkryl=req.nkryl,
-                                linsys_tol=req.linsys_tol, linsys_max=req.linsys_max, temperature=req.temperature)
+                                linsys_tol=req.linsys_tol, linsys_max=req.linsys_max, temperature=req.temperature,
+                                per_gs=True)
         results = []
         for (r, _), om in zip(group, oms):
             idx = np.searchsorted(allw, om)
             cols = [pins.index(siam_pol_in(p)) * len(pouts) + pouts.index(siam_pol_out(p)) for p in r.pols]
-            results.append({"omegas": om, "spectra": out.spectra[idx][:, :, cols], "coalesced": len(group),
-                            "minres_iters": out.iters})
+            w = rixs.boltz(res.gs_e[:r.ngs], r.temperature)  # this request's own ground states
+            spec = np.einsum("weng,g->wen", out.spectra_gs[idx][:, :, cols, :r.ngs], w)
+            results.append({"omegas": om, "spectra": spec, "coalesced": len(group), "minres_iters": out.iters})
         return results
 
-    def _xas(self, r: Request, res: Resident):
-        D = res.op("xas", r.pols[0])
-        phi = device.spmm(D, res.gs_v[:, :r.ngs].contiguous())
+    def _xas_group(self, group, res: Resident):
+        """XAS of every request in the group from one Krylov launch: the start vectors
+        D_xas(pol)|g> of all of them side by side (build_krylov_mp per column, as the
+        reference runs them one by one), then each request's continued fraction."""
+        phis, spans = [], []
+        c0 = 0
+        for r, _ in group:
+            phis.append(device.spmm(res.op("xas", r.pols[0]), res.gs_v[:, :r.ngs].contiguous()))
+            spans.append((c0, c0 + r.ngs))
+            c0 += r.ngs
+        phi = torch.cat(phis, dim=1).contiguous()
         pk = res.packed.get("hn")
-        kr = device.krylov(res.Hn, phi, r.nkryl, apply=dict(packed=pk) if pk is not None else None)
-        w = rixs.boltz(res.gs_e[:r.ngs], r.temperature)
-        grid = np.asarray(r.eloss, dtype=np.float64) + res.edge
-        spec = device.cf_spectrum(kr.neff, kr.alpha, kr.beta, res.gs_e[:r.ngs], kr.norm.cpu().numpy(), w, grid,
-                                  np.full(len(grid), r.gamma_c))
-        return {"grid": grid, "spectrum": spec.cpu().numpy()}
+        kr = device.krylov(res.Hn, phi, group[0][0].nkryl, apply=dict(packed=pk) if pk is not None else None)
+        norm = kr.norm.cpu().numpy()
+        out = []
+        for (r, _), (a, b) in zip(group, spans):
+            w = rixs.boltz(res.gs_e[:r.ngs], r.temperature)
+            grid = np.asarray(r.eloss, dtype=np.float64) + res.edge
+            spec = device.cf_spectrum(kr.neff[a:b], kr.alpha[a:b], kr.beta[a:b], res.gs_e[:r.ngs], norm[a:b], w,
+                                      grid, np.full(len(grid), r.gamma_c))
+            out.append({"grid": grid, "spectrum": spec.cpu().numpy(), "coalesced": len(group)})
+        return out
 
 
 def _warm_torch():

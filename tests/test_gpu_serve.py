@@ -40,6 +40,41 @@ def test_alone_vs_mix(cuda):
     assert summ["n"] == 6 and summ["p99_ms"] >= summ["p50_ms"] > 0
 
 
+def test_coalesced_requests_match_alone(cuda):
+    """Requests that wait while the only worker is busy join one solve: RIXS with different
+    ground-state counts, polarisations and incident energies, and XAS with different
+    polarisations.  Each gets the result it gets alone, within 1e-6."""
+    from edrixs_b200.serve import ModelSpec, Request, Server
+    m1 = ModelSpec(2, 3, 21)
+    eloss = np.linspace(-0.5, 8.0, 400)
+
+    def rixs_req(oms, ngs, pols):
+        return Request("rixs", m1, ngs=ngs, omegas=np.asarray(oms), eloss=eloss, gamma_c=0.6, gamma_f=0.1,
+                       pols=pols, nkryl=60)
+
+    def xas_req(pol, ngs):
+        return Request("xas", m1, ngs=ngs, eloss=np.linspace(-3, 12, 300), gamma_c=0.3, pols=(pol,), nkryl=80)
+
+    reqs = [lambda: rixs_req([0.5, 2.0], 1, (1,)), lambda: rixs_req([1.0, 2.0, 6.0], 2, (0, 3)),
+            lambda: xas_req(0, 1), lambda: xas_req(1, 2)]
+    srv = Server(hbm_budget=40e9, workers=1).start()
+    try:
+        alone = [srv.submit(f()).result(timeout=600) for f in reqs]
+        # keep the one worker busy, then queue all four: they wait and are grouped
+        busy = srv.submit(Request("ed", ModelSpec(6, 8, 5), ngs=3))
+        futs = [srv.submit(f()) for f in reqs]
+        busy.result(timeout=600)
+        mix = [f.result(timeout=600) for f in futs]
+    finally:
+        srv.shutdown()
+    assert mix[0]["coalesced"] == 2 and mix[2]["coalesced"] == 2
+    for a, b in zip(alone[:2], mix[:2]):
+        assert b["spectra"].shape == a["spectra"].shape
+        assert rel_linf(b["spectra"], a["spectra"]) < 1e-6
+    for a, b in zip(alone[2:], mix[2:]):
+        assert rel_linf(b["spectrum"], a["spectrum"]) < 1e-6
+
+
 def test_failed_request_does_not_stop_server(cuda):
     from edrixs_b200.serve import ModelSpec, Request, Server
     srv = Server(hbm_budget=40e9, workers=2).start()

@@ -25,3 +25,19 @@ def test_serve_mix_is_seeded_and_in_range():
         assert math.comb(norb, r.model.nelec) <= 705432
     kinds = {r.kind for _, r in a}
     assert kinds == {"ed", "xas", "rixs"}
+
+
+def test_coalesce_key_groups_compatible_requests():
+    from edrixs_b200.serve import ModelSpec, Request, coalesce_key
+    m, m2 = ModelSpec(4, 7, 1), ModelSpec(4, 7, 2)
+    el = np.linspace(-0.5, 12.0, 1000)
+    a = Request("rixs", m, ngs=1, omegas=np.array([1.0]), eloss=el, pols=(0,))
+    b = Request("rixs", m, ngs=3, omegas=np.array([2.0, 3.0]), eloss=el.copy(), pols=(1, 2))
+    assert coalesce_key(a) == coalesce_key(b)
+    assert coalesce_key(a) != coalesce_key(Request("rixs", m2, omegas=np.array([1.0]), eloss=el))
+    assert coalesce_key(a) != coalesce_key(Request("rixs", m, omegas=np.array([1.0]), eloss=el[:500]))
+    assert coalesce_key(a) != coalesce_key(Request("rixs", m, omegas=np.array([1.0]), eloss=el, gamma_f=0.3))
+    x1 = Request("xas", m, ngs=1, eloss=el, pols=(0,), nkryl=200)
+    x2 = Request("xas", m, ngs=2, eloss=el[:10], pols=(1,), nkryl=200)
+    assert coalesce_key(x1) == coalesce_key(x2) != coalesce_key(a)
+    assert coalesce_key(Request("ed", m)) is None

@@ -59,7 +59,7 @@ __global__ void k_mr_scale(int64_t n, double2* __restrict__ v, MinresState* S, i
 }
 
 // tmp = op(A) v, alpha = <v, tmp>
-template <class VT>
+template <class VT, int HALF>
 __global__ void __launch_bounds__(MT) k_mr_apply(int64_t n, const int64_t* __restrict__ row_ptr,
                                                  const int32_t* __restrict__ col, const VT* __restrict__ val,
                                                  double2 aop, double2 sop, const double2* __restrict__ v,
@@ -69,8 +69,8 @@ __global__ void __launch_bounds__(MT) k_mr_apply(int64_t n, const int64_t* __res
     double pr = 0.0, pi = 0.0;
     const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    spmv_rows<VT, double2>(w0, n, nw, row_ptr, col, val, v, 1, 0, [&](int64_t r, double2 acc) {
-        if (lane == 0) {
+    auto epi = [&](int64_t r, double2 acc) {
+        if ((lane & (HALF > 0 ? 15 : 31)) == 0) {  // the row's leading lane
             double2 vr = v[r];
             double2 t = cmul(aop, acc);
             if (sop.x != 0.0 || sop.y != 0.0) t = cadd(t, cmul(sop, vr));
@@ -78,7 +78,11 @@ __global__ void __launch_bounds__(MT) k_mr_apply(int64_t n, const int64_t* __res
             pr += vr.x * t.x + vr.y * t.y;
             pi += vr.x * t.y - vr.y * t.x;
         }
-    });
+    };
+    if constexpr (HALF > 0)  // rows of <= ~100 entries: two per warp
+        spmv_rows_half<HALF, VT, double2>(w0, nw, n, row_ptr, col, val, v, 1, 0, epi);
+    else
+        spmv_rows<VT, double2>(w0, n, nw, row_ptr, col, val, v, 1, 0, epi);
     double sr = block_sum(pr);
     double si = block_sum(pi);
     if (threadIdx.x == 0) {
@@ -332,22 +336,36 @@ extern "C" int edx_minres(const edx_csr* A, double alpha_re, double alpha_im, do
     EDX_CHECK_LAUNCH();
     const double2 aop = make_double2(alpha_re, alpha_im), sop = make_double2(sigma_re, sigma_im);
     // the SpMV runs as one wave of resident blocks (at most 8 per SM: the partials buffer)
+    // two rows per warp for rows of <= 100 entries on average, with 5 entries per lane
+    // prefetched up to 75 (see spmv_rows_half)
+    const int half = A->nnz <= 100 * n ? (A->nnz <= 75 * n ? 5 : 6) : 0;
     int res = 4;
     if (A->val_type == EDX_C128)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, k_mr_apply<double2>, MT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, half ? k_mr_apply<double2, 6> : k_mr_apply<double2, 0>, MT,
+                                                      0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, k_mr_apply<float2>, MT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res, half ? k_mr_apply<float2, 6> : k_mr_apply<float2, 0>, MT,
+                                                      0);
     res = std::max(1, std::min(res, 8));
-    const int ga = (int)std::min<int64_t>((n * 32 + MT - 1) / MT, (int64_t)num_sms() * res);
+    const int64_t warps = half ? (n + 1) / 2 : n;
+    const int ga = (int)std::min<int64_t>((warps * 32 + MT - 1) / MT, (int64_t)num_sms() * res);
     const int poll = 8;
     for (int it = 0; it < maxit; ++it) {
         k_mr_scale<<<g, MT, 0, st>>>(n, vc, S, it);
-        if (A->val_type == EDX_C128)
-            k_mr_apply<double2><<<ga, MT, 0, st>>>(n, A->row_ptr, A->col, reinterpret_cast<const double2*>(A->val),
-                                                   aop, sop, vc, tmp, part, S, it);
+        const double2* v2 = reinterpret_cast<const double2*>(A->val);
+        const float2* v1 = reinterpret_cast<const float2*>(A->val);
+        if (A->val_type == EDX_C128 && half == 5)
+            k_mr_apply<double2, 5><<<ga, MT, 0, st>>>(n, A->row_ptr, A->col, v2, aop, sop, vc, tmp, part, S, it);
+        else if (A->val_type == EDX_C128 && half == 6)
+            k_mr_apply<double2, 6><<<ga, MT, 0, st>>>(n, A->row_ptr, A->col, v2, aop, sop, vc, tmp, part, S, it);
+        else if (A->val_type == EDX_C128)
+            k_mr_apply<double2, 0><<<ga, MT, 0, st>>>(n, A->row_ptr, A->col, v2, aop, sop, vc, tmp, part, S, it);
+        else if (half == 5)
+            k_mr_apply<float2, 5><<<ga, MT, 0, st>>>(n, A->row_ptr, A->col, v1, aop, sop, vc, tmp, part, S, it);
+        else if (half == 6)
+            k_mr_apply<float2, 6><<<ga, MT, 0, st>>>(n, A->row_ptr, A->col, v1, aop, sop, vc, tmp, part, S, it);
         else
-            k_mr_apply<float2><<<ga, MT, 0, st>>>(n, A->row_ptr, A->col, reinterpret_cast<const float2*>(A->val),
-                                                  aop, sop, vc, tmp, part, S, it);
+            k_mr_apply<float2, 0><<<ga, MT, 0, st>>>(n, A->row_ptr, A->col, v1, aop, sop, vc, tmp, part, S, it);
         k_mr_orth<<<g, MT, 0, st>>>(n, vc, vp, tmp, part, S, it, tol, maxit);
         k_mr_update<<<g, MT, 0, st>>>(n, vc, wp, wc, x, S, it);
         EDX_CHECK_LAUNCH();

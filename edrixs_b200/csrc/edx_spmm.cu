@@ -40,7 +40,7 @@ __device__ __forceinline__ void row_times_x_slot(int64_t start, int64_t end, con
     }
 }
 
-template <int KW, class VT, class XT, bool ROWSLOT>
+template <int KW, class VT, class XT, bool ROWSLOT, int HALF = 0>
 __global__ void __launch_bounds__(256) k_spmm(int64_t nrows, const int64_t* __restrict__ row_ptr,
                                               const int32_t* __restrict__ col, const VT* __restrict__ val,
                                               int k, const XT* __restrict__ X, int64_t ldx_, XT* __restrict__ Y,
@@ -74,48 +74,75 @@ __global__ void __launch_bounds__(256) k_spmm(int64_t nrows, const int64_t* __re
         out.y = yi;
         *yp = out;
     };
-    if (KW == 1 && !ROWSLOT) {  // one column, long rows: the next row loads during this one
+    if constexpr (KW == 1 && !ROWSLOT && HALF > 0) {  // one column, rows of <= ~100 entries: two per warp
+        spmv_rows_half<HALF, VT, XT>(warp0, nw, nrows, row_ptr, col, val, X, ldx_, gc, [&](int64_t r, AT acc) {
+            if ((lane & 15) == 0) store(r, acc);
+        });
+        return;
+    } else if constexpr (KW == 1 && !ROWSLOT) {  // one column, long rows: the next row loads during this one
         spmv_rows<VT, XT>(warp0, nrows, nw, row_ptr, col, val, X, ldx_, gc, [&](int64_t r, AT acc) {
             if (lane == 0) store(r, acc);
         });
         return;
-    }
-    const int64_t rstep = ROWSLOT ? nw * SLOTS : nw;
-    for (int64_t rb = ROWSLOT ? warp0 * SLOTS : warp0; rb < nrows; rb += rstep) {
-        const int64_t r = ROWSLOT ? rb + slot : rb;
-        AT acc;
-        bool mine;
-        if (ROWSLOT) {
-            mine = slot < SLOTS && r < nrows;
-            const int64_t s = mine ? __ldg(row_ptr + r) : 0, e = mine ? __ldg(row_ptr + r + 1) : 0;
-            row_times_x_slot<KW, VT, XT>(s, e, col, val, X, ldx_, gc, colok, acc);
-        } else {
-            mine = lane < KW;
-            const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
-            AT accv[1];
-            row_times_x_tiles<KW, 1, VT, XT>(s, e, col, val, X, ldx_, blockIdx.y * KW, k, accv);
-            acc = accv[0];
+    } else {
+        const int64_t rstep = ROWSLOT ? nw * SLOTS : nw;
+        for (int64_t rb = ROWSLOT ? warp0 * SLOTS : warp0; rb < nrows; rb += rstep) {
+            const int64_t r = ROWSLOT ? rb + slot : rb;
+            AT acc;
+            bool mine;
+            if (ROWSLOT) {
+                mine = slot < SLOTS && r < nrows;
+                const int64_t s = mine ? __ldg(row_ptr + r) : 0, e = mine ? __ldg(row_ptr + r + 1) : 0;
+                row_times_x_slot<KW, VT, XT>(s, e, col, val, X, ldx_, gc, colok, acc);
+            } else {
+                mine = lane < KW;
+                const int64_t s = __ldg(row_ptr + r), e = __ldg(row_ptr + r + 1);
+                AT accv[1];
+                row_times_x_tiles<KW, 1, VT, XT>(s, e, col, val, X, ldx_, blockIdx.y * KW, k, accv);
+                acc = accv[0];
+            }
+            if (mine && colok) store(r, acc);
         }
-        if (mine && colok) store(r, acc);
     }
 }
 
 // rows of at most this many entries on average run one row per slot
 constexpr int64_t SHORT_ROW = 16;
+// one-column products on rows of at most this many entries on average run two rows per warp
+constexpr int64_t HALF_WARP_ROW = 100;
+constexpr int64_t HALF_NC5_ROW = 75;  // up to this many: five entries per lane prefetched, else six
 
 // resident blocks per SM of a kernel (cached per device): a grid-stride launch then runs as
 // one wave with no tail of late blocks
-template <class K>
-static int resident_blocks(K kern, int threads) {
+// (one cache per kernel: the kernel is a template argument, so that instantiations with the
+// same signature do not share an entry)
+template <auto KERN>
+static int resident_blocks(int threads) {
     static int cache[EDX_MAX_DEVICES] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= EDX_MAX_DEVICES) return 4;
     if (cache[dev] == 0) {
         int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, threads, 0) != cudaSuccess || nb < 1) nb = 4;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, KERN, threads, 0) != cudaSuccess || nb < 1) nb = 4;
         cache[dev] = nb;
     }
     return cache[dev];
+}
+
+template <int NC, class VT, class XT>
+static int launch_spmv_half(const edx_csr* A, const void* x, int64_t ldx_, void* y, int64_t ldy, int64_t ycs,
+                            double2 al, double2 sg, double2 be, cudaStream_t st) {
+    const int threads = 256;
+    const int res = resident_blocks<k_spmm<1, VT, XT, false, NC>>(threads);
+    const int64_t need = ((A->nrows + 1) / 2 * 32 + threads - 1) / threads;
+    const int64_t bx = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)num_sms() * res));
+    const int hs = (sg.x != 0.0 || sg.y != 0.0) ? 1 : 0;
+    const int hb = (be.x != 0.0 || be.y != 0.0) ? 1 : 0;
+    k_spmm<1, VT, XT, false, NC><<<dim3((unsigned)bx, 1), threads, 0, st>>>(
+        A->nrows, A->row_ptr, A->col, reinterpret_cast<const VT*>(A->val), 1, reinterpret_cast<const XT*>(x), ldx_,
+        reinterpret_cast<XT*>(y), ldy, ycs, al, sg, be, hs, hb);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
 }
 
 template <int KW, class VT, class XT>
@@ -123,10 +150,15 @@ static int launch_spmm_t(const edx_csr* A, int k, const void* x, int64_t ldx_, v
                          int64_t ycs, double2 al, double2 sg, double2 be, cudaStream_t st) {
     const int threads = 256;
     const bool rowslot = KW < 32 && A->nnz <= SHORT_ROW * A->nrows;
+    if (KW == 1 && !rowslot && A->nnz <= HALF_WARP_ROW * A->nrows) {  // two rows per warp
+        if (A->nnz <= HALF_NC5_ROW * A->nrows) return launch_spmv_half<5, VT, XT>(A, x, ldx_, y, ldy, ycs, al, sg, be, st);
+        return launch_spmv_half<6, VT, XT>(A, x, ldx_, y, ldy, ycs, al, sg, be, st);
+    }
+
     const int64_t rows_per_warp = rowslot ? 32 / KW : 1;
     int64_t need = ((A->nrows + rows_per_warp - 1) / rows_per_warp * 32 + threads - 1) / threads;
-    const int res = rowslot ? resident_blocks(k_spmm<KW, VT, XT, true>, threads)
-                            : resident_blocks(k_spmm<KW, VT, XT, false>, threads);
+    const int res = rowslot ? resident_blocks<k_spmm<KW, VT, XT, true>>(threads)
+                            : resident_blocks<k_spmm<KW, VT, XT, false>>(threads);
     int64_t maxb = (int64_t)num_sms() * res;
     int64_t bx = need < maxb ? need : maxb;
     if (bx < 1) bx = 1;

@@ -221,3 +221,18 @@ def test_wide_packed_krylov_matches_csr(cuda, k):
     assert torch.equal(p.neff, c.neff)
     assert torch.allclose(p.alpha, c.alpha, rtol=1e-10, atol=1e-10)
     assert torch.allclose(p.beta, c.beta, rtol=1e-10, atol=1e-10)
+
+
+def test_pack_diagonal_only_matrix(cuda):
+    """No off-diagonal entries: an empty value table, and the product is the diagonal alone."""
+    import torch
+    from edrixs_b200 import device
+    n = 1000
+    d = torch.complex(torch.linspace(-1, 1, n, dtype=torch.float64), torch.linspace(0, 2, n, dtype=torch.float64))
+    A = device.CSR(torch.arange(n + 1, dtype=torch.int64, device="cuda"),
+                   torch.arange(n, dtype=torch.int32, device="cuda"), d.cuda(), n)
+    P = device.pack(A)
+    assert P is not None and P.nnz == 0 and P.vals.numel() == 0
+    _assert_pack_lossless(P, A)
+    X = torch.randn((n, 3), dtype=torch.float64, device="cuda").to(torch.complex128)
+    assert torch.allclose(device.spmm(P, X), d.cuda()[:, None] * X, rtol=0, atol=1e-15)

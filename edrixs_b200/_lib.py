@@ -63,7 +63,8 @@ class KrylovOpts(ctypes.Structure):
                 ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int),
                 ("apply_layout", ctypes.POINTER(Tiles)), ("apply_packed", ctypes.POINTER(Packed)),
                 ("proj_window", ctypes.c_int), ("nacc", ctypes.c_int), ("acc_col", vp), ("acc_coef", vp),
-                ("acc_out", ctypes.POINTER(vp)), ("acc_ld", i64), ("v0_ld", i64)]
+                ("acc_out", ctypes.POINTER(vp)), ("acc_ld", i64), ("v0_ld", i64),
+                ("apply_rowslot", ctypes.c_int)]
 
 
 _SIGS = {

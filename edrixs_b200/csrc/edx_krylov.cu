@@ -244,6 +244,87 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_lanczos_apply_packed(int64_t 
     }
 }
 
+// ---- K9a on the packed form, one row per slot ------------------------------------------------
+// For a few columns (k <= 16): each slot of KW lanes walks a row of its own, U entries at a
+// time (the slot's lanes read the same word, then gather their own columns), so no
+// cross-slot reduction runs per row and no lanes idle at the end of a row.  Rows of the
+// block's warps are consecutive: warp w's slot q takes row (b*NW + w)*SLOTS + q of the
+// sweep.  The epilogue and the alpha partials are those of k_lanczos_apply_packed.
+template <int KW, int NT, bool WIDE>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_lanczos_apply_packed_rs(int64_t n, PackedView M,
+                                                                            const double2* __restrict__ Vc,
+                                                                            double2* __restrict__ Vp, KrylovState S,
+                                                                            int it) {
+    constexpr int NW = NT / 32;
+    constexpr int SLOTS = 32 / KW;
+    constexpr int U = 4;
+    extern __shared__ double2 rs_tab[];
+    __shared__ double sh[NW * KW];
+    for (int i = threadIdx.x; i < M.nval; i += NT) rs_tab[i] = M.vals[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KW, c = lane % KW;
+    const int k = S.k;
+    const bool mine = slot < SLOTS && c < k;
+    const uint32_t vmask = WIDE ? 0u : (1u << M.vbits) - 1u;
+    const double bprev = (mine && it > 0) ? S.beta[c] * S.sprev[c] : 0.0;
+    const double scur = mine ? S.scur[c] : 0.0;
+    double apart = 0.0;
+    const int64_t rstep = (int64_t)gridDim.x * NW * SLOTS;
+    for (int64_t rb = ((int64_t)blockIdx.x * NW + warp) * SLOTS; rb < n; rb += rstep) {
+        const int64_t r = rb + slot;
+        const bool live = slot < SLOTS && r < n;
+        const int64_t s = live ? __ldg(M.row_ptr + r) : 0, e = live ? __ldg(M.row_ptr + r + 1) : 0;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int64_t j0 = s; j0 < e; j0 += U) {
+            double2 v[U], x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t j = j0 + u;
+                const bool ok = j < e;
+                int64_t cc = 0;
+                uint32_t q = 0;
+                if (ok) pk_decode<WIDE>(__ldg(M.ent + j), WIDE ? (uint32_t)__ldg(M.vidx + j) : 0u, M.vbits, vmask, cc, q);
+                v[u] = ok ? rs_tab[q] : make_double2(0.0, 0.0);
+                x[u] = (ok && c < k) ? ldx(Vc + cc * k + c) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc = fma_c(v[u], x[u], acc);
+        }
+        if (live && c < k) {
+            const int64_t o = r * k + c;
+            const double2 vc = Vc[o];
+            const double2 hv = fma_c(__ldg(M.diag + r), vc, acc);
+            const double2 vp = Vp[o];
+            double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
+            w.x = w.x + scur * hv.x;
+            w.y = w.y + scur * hv.y;
+            Vp[o] = w;
+            apart += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
+        }
+    }
+    // the slots' partials of each column, then the block's
+    double tot = 0.0;
+#pragma unroll
+    for (int q = 0; q < SLOTS; ++q) tot += __shfl_sync(0xffffffffu, apart, q * KW + (lane % KW));
+    if (lane < KW) sh[warp * KW + lane] = tot;
+    __syncthreads();
+    for (int i = threadIdx.x; i < KW; i += NT) {
+        double t = 0.0;
+        for (int w = 0; w < NW; ++w) t += sh[w * KW + i];
+        if (i < k) S.part[(int64_t)blockIdx.x * k + i] = t;
+    }
+    __syncthreads();
+    if (arrive_last(S.ticket)) {
+        for (int j = threadIdx.x; j < k; j += NT) {
+            const double a = S.scur[j] * sum_partials(S.part, gridDim.x, k, j);
+            S.alpha[j] = a;
+            if (S.active[j]) S.alpha_out[(int64_t)j * S.maxn + it] = a;
+        }
+        if (threadIdx.x == 0) *S.ticket = 0u;
+    }
+}
+
 // ---- K9a on the tiled layout ------------------------------------------------------------
 // One block per (row tile, 32 columns).  The block walks the pieces of its row tile; for
 // each piece it stages the column tile of V_cur (32 columns, up to EDX_TILE_COLS_MAX rows)
@@ -679,6 +760,7 @@ struct ApplyCfg {
     int gx;         // blocks along the rows
     int chunked;    // contiguous row ranges per block
     int prefetch;   // bulk-prefetch each warp's next row into L2
+    int rowslot;    // packed form, k <= kw <= 16: one row per slot (k_lanczos_apply_packed_rs)
 };
 
 template <int KW, int TG, class VT, int NT>
@@ -762,11 +844,52 @@ static int launch_packed(int64_t n, const PackedView& M, const double2* Vc, doub
     return launch_packed_nt<KW, TG, 256, false>(n, M, Vc, Vp, S, it, cfg, st);
 }
 
+template <int KW, int NT, bool WIDE>
+static int launch_packed_rs_nt(int64_t n, const PackedView& M, const double2* Vc, double2* Vp, const KrylovState& S,
+                               int it, const ApplyCfg& cfg, cudaStream_t st) {
+    auto kern = k_lanczos_apply_packed_rs<KW, NT, WIDE>;
+    static bool attr_set[EDX_MAX_DEVICES] = {};
+    int dev = 0;
+    EDX_CUDA(cudaGetDevice(&dev));
+    EDX_REQUIRE(dev >= 0 && dev < EDX_MAX_DEVICES, "edx_krylov: device ordinal %d out of range", dev);
+    if (!attr_set[dev]) {
+        EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(EDX_PACK_VALUES_MAX * sizeof(double2))));
+        attr_set[dev] = true;
+    }
+    kern<<<cfg.gx, NT, (size_t)M.nval * sizeof(double2), st>>>(n, M, Vc, Vp, S, it);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}
+
+template <int KW>
+static int launch_packed_rs(int64_t n, const PackedView& M, const double2* Vc, double2* Vp, const KrylovState& S,
+                            int it, const ApplyCfg& cfg, cudaStream_t st) {
+    if (M.vbits == 0) {
+        if (cfg.threads == 1024) return launch_packed_rs_nt<KW, 1024, true>(n, M, Vc, Vp, S, it, cfg, st);
+        return launch_packed_rs_nt<KW, 256, true>(n, M, Vc, Vp, S, it, cfg, st);
+    }
+    if (cfg.threads == 1024) return launch_packed_rs_nt<KW, 1024, false>(n, M, Vc, Vp, S, it, cfg, st);
+    return launch_packed_rs_nt<KW, 256, false>(n, M, Vc, Vp, S, it, cfg, st);
+}
+
 static int apply_packed(const edx_packed* P, const double2* Vc, double2* Vp, const KrylovState& S, int it,
                         const ApplyCfg& cfg, cudaStream_t st) {
     const PackedView M{P->row_ptr, P->ent, reinterpret_cast<const double2*>(P->vals),
                        reinterpret_cast<const double2*>(P->diag), P->vbits, P->nval, P->vidx};
     const int64_t n = P->nrows;
+    if (cfg.rowslot) {
+        switch (cfg.kw) {
+        case 1: return launch_packed_rs<1>(n, M, Vc, Vp, S, it, cfg, st);
+        case 2: return launch_packed_rs<2>(n, M, Vc, Vp, S, it, cfg, st);
+        case 4: return launch_packed_rs<4>(n, M, Vc, Vp, S, it, cfg, st);
+        case 6: return launch_packed_rs<6>(n, M, Vc, Vp, S, it, cfg, st);
+        case 8: return launch_packed_rs<8>(n, M, Vc, Vp, S, it, cfg, st);
+        case 12: return launch_packed_rs<12>(n, M, Vc, Vp, S, it, cfg, st);
+        case 16: return launch_packed_rs<16>(n, M, Vc, Vp, S, it, cfg, st);
+        }
+        return fail(EDX_ERR_INVALID, "krylov: one row per slot needs a column group of at most 16");
+    }
     switch (cfg.kw) {
     case 1: return launch_packed<1, 1>(n, M, Vc, Vp, S, it, cfg, st);
     case 2: return launch_packed<2, 1>(n, M, Vc, Vp, S, it, cfg, st);
@@ -926,6 +1049,7 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     const int bps = (opts && opts->apply_blocks_per_sm > 0) ? opts->apply_blocks_per_sm : 1;
     cfg.chunked = (opts && opts->apply_chunked > 0) ? 1 : 0;
     cfg.prefetch = (opts && opts->apply_prefetch > 0) ? 1 : 0;
+    cfg.rowslot = (opts && opts->apply_rowslot > 0) ? 1 : 0;
     const int ntiles = (k + cfg.kw - 1) / cfg.kw;
     cfg.tg = (opts && opts->apply_tiles > 0) ? opts->apply_tiles : (ntiles >= 4 ? 4 : (ntiles >= 2 ? 2 : 1));
     if (cfg.kw < 16) cfg.tg = 1;
@@ -953,6 +1077,9 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
                         (packed->vbits > 0 || packed->nnz == 0 || packed->vidx),
                     "edx_krylov: apply_packed does not describe this matrix");
     }
+    if (cfg.rowslot)
+        EDX_REQUIRE(packed && !layout && cfg.kw <= 16 && k <= cfg.kw,
+                    "edx_krylov: apply_rowslot needs the packed form and k <= apply_col_group <= 16");
     const int kw = pow2_kw(k);  // layout of the element-wise recurrence kernels
     const int gy = (k + kw - 1) / kw;
     int gx = num_sms() * 8;

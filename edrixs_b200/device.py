@@ -493,6 +493,7 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
         opts.apply_chunked = int(apply.get("chunked", 0))
         opts.apply_tiles = int(apply.get("tiles", 0))
         opts.apply_prefetch = int(apply.get("prefetch", 0))
+        opts.apply_rowslot = int(apply.get("rowslot", 0))
         if apply.get("layout") is not None:
             tdesc = apply["layout"].desc()
             opts.apply_layout = ctypes.pointer(tdesc)

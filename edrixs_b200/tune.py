@@ -51,6 +51,8 @@ def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None,
     cands = candidates(k)
     if packed is not None and not c64:
         cands = cands + [dict(c, packed=1) for c in candidates(k)]
+        if k <= 16:  # one row per lane group
+            cands += [dict(c, packed=1, rowslot=1) for c in candidates(k) if c["chunked"] == 0]
     if layout is not None and not c64:
         cands = [dict(tiled=1)] + cands
 

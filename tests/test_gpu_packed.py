@@ -106,7 +106,9 @@ def test_packed_krylov_matches_oracle(cuda, k):
 @pytest.mark.parametrize("shape", [dict(col_group=6, threads=1024, blocks_per_sm=1, chunked=0),
                                    dict(col_group=8, threads=256, blocks_per_sm=4, chunked=1),
                                    dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1, chunked=0),
-                                   dict(col_group=16, tiles=4, threads=256, blocks_per_sm=8, chunked=1)])
+                                   dict(col_group=16, tiles=4, threads=256, blocks_per_sm=8, chunked=1),
+                                   dict(col_group=6, threads=1024, blocks_per_sm=1, rowslot=1),
+                                   dict(col_group=8, threads=256, blocks_per_sm=4, rowslot=1)])
 def test_packed_launch_shapes_agree(cuda, shape):
     import torch
     from edrixs_b200 import device
@@ -236,3 +238,30 @@ def test_pack_diagonal_only_matrix(cuda):
     _assert_pack_lossless(P, A)
     X = torch.randn((n, 3), dtype=torch.float64, device="cuda").to(torch.complex128)
     assert torch.allclose(device.spmm(P, X), d.cuda()[:, None] * X, rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("form", ["narrow", "wide"])
+def test_rowslot_apply_matches_oracle(cuda, form):
+    """One row per lane group (apply_rowslot) on both packed forms: Lanczos coefficients of
+    the oracle to its tolerance, with shifts and projections as the batched RIXS runs them."""
+    import torch
+    from edrixs_b200 import device
+    ref, gpu = _ham("ham_i")
+    P = device.pack(gpu, form=form)
+    rng = np.random.default_rng(12)
+    k, maxn = 3, 40
+    V0 = rng.normal(size=(ref.nrows, k)) + 1j * rng.normal(size=(ref.nrows, k))
+    Vt = torch.from_numpy(V0).cuda()
+    shifts = (np.array([0, 1, 2]), np.array([-30 + 0.5j, -28 + 1j, -31 + 0.3j]))
+    a = device.krylov(gpu, Vt, maxn, proj=[gpu], shifts=shifts)
+    b = device.krylov(gpu, Vt, maxn, proj=[gpu], shifts=shifts,
+                      apply=dict(col_group=4, threads=256, blocks_per_sm=4, rowslot=1, packed=P))
+    assert torch.equal(a.shift_iters, b.shift_iters)
+    assert torch.allclose(a.alpha, b.alpha, rtol=1e-10, atol=1e-10)
+    assert torch.allclose(a.shift_y, b.shift_y, rtol=1e-9, atol=1e-12)
+    for j in range(k):  # the shifts stop the recurrence once they converge: compare that many steps
+        n0 = b.neff[j].item()
+        al, be, nrm, neff = orc.build_krylov(ref, V0[:, j], n0)
+        assert neff == n0
+        assert np.allclose(b.alpha[j].cpu().numpy()[:n0], al, rtol=1e-8, atol=1e-8)
+        assert np.allclose(b.beta[j].cpu().numpy()[:n0], be, rtol=1e-8, atol=1e-8)

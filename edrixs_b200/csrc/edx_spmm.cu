@@ -231,8 +231,9 @@ int spmm_dispatch(const edx_csr* A, int k, int vec_type, const void* x, int64_t 
 }
 
 // ---- the same product on the packed form ----------------------------------------------
-// Warp per row (slots of KW lanes share the row's entries), value table in shared memory,
-// diagonal term added with the store.
+// Value table in shared memory, diagonal term added with the store.  One column: warp per
+// row with the next row's words prefetched; up to 16 columns per tile: one row per group of
+// KW lanes; 32: warp per row.
 template <int KW, bool WIDE>
 __global__ void __launch_bounds__(256) k_spmm_packed(int64_t nrows, PackedView M, int k, const double2* __restrict__ X,
                                                      int64_t ldx_, double2* __restrict__ Y, int64_t ldy,
@@ -268,6 +269,35 @@ __global__ void __launch_bounds__(256) k_spmm_packed(int64_t nrows, PackedView M
         spmv_rows_packed<WIDE>(warp0, nrows, nw, M, sp_tab, X, ldx_, col0, [&](int64_t r, double2 acc) {
             if (lane == 0) store(r, acc);
         });
+    } else if constexpr (KW <= 16) {  // a few columns: each lane group walks a row of its own
+        constexpr int SLOTS = 32 / KW;
+        constexpr int U = 4;
+        const int slot = lane / KW;
+        const uint32_t vmask = WIDE ? 0u : (1u << M.vbits) - 1u;
+        for (int64_t rb = warp0 * SLOTS; rb < nrows; rb += nw * SLOTS) {
+            const int64_t r = rb + slot;
+            const bool live = slot < SLOTS && r < nrows;
+            const int64_t s = live ? __ldg(M.row_ptr + r) : 0, e = live ? __ldg(M.row_ptr + r + 1) : 0;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int64_t j0 = s; j0 < e; j0 += U) {
+                double2 v[U], xv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int64_t j = j0 + u;
+                    const bool ok = j < e;
+                    int64_t cc = 0;
+                    uint32_t q = 0;
+                    if (ok)
+                        pk_decode<WIDE>(__ldg(M.ent + j), WIDE ? (uint32_t)__ldg(M.vidx + j) : 0u, M.vbits, vmask, cc,
+                                        q);
+                    v[u] = ok ? sp_tab[q] : make_double2(0.0, 0.0);
+                    xv[u] = (ok && gc < k) ? ldx(X + cc * ldx_ + gc) : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) acc = fma_c(v[u], xv[u], acc);
+            }
+            if (live && gc < k) store(r, acc);
+        }
     } else {
         for (int64_t r = warp0; r < nrows; r += nw) {
             const int64_t s = __ldg(M.row_ptr + r), e = __ldg(M.row_ptr + r + 1);

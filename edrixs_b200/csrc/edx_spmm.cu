@@ -149,7 +149,10 @@ template <int KW, class VT, class XT>
 static int launch_spmm_t(const edx_csr* A, int k, const void* x, int64_t ldx_, void* y, int64_t ldy,
                          int64_t ycs, double2 al, double2 sg, double2 be, cudaStream_t st) {
     const int threads = 256;
-    const bool rowslot = KW < 32 && A->nnz <= SHORT_ROW * A->nrows;
+    // a row per slot for short rows at any width below 32, and for 6-16 columns at any row
+    // length: no reduction across slots per row (H_n, 6 columns: 1.13 ms against 1.65 ms with
+    // a warp per row; at 3 columns the two were level)
+    const bool rowslot = KW < 32 && (A->nnz <= SHORT_ROW * A->nrows || (KW >= 6 && KW <= 16));
     if (KW == 1 && !rowslot && A->nnz <= HALF_WARP_ROW * A->nrows) {  // two rows per warp
         if (A->nnz <= HALF_NC5_ROW * A->nrows) return launch_spmv_half<5, VT, XT>(A, x, ldx_, y, ldy, ycs, al, sg, be, st);
         return launch_spmv_half<6, VT, XT>(A, x, ldx_, y, ldy, ycs, al, sg, be, st);

@@ -325,6 +325,62 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_lanczos_apply_packed_rs(int64
     }
 }
 
+// ---- K9a on the CSR, one row per slot (k <= KW <= 16) --------------------------------------
+// As k_lanczos_apply_packed_rs, with the entries read from the CSR (row_times_x_slot).
+template <int KW, class VT, int NT>
+__global__ void __launch_bounds__(NT) k_lanczos_apply_rs(int64_t n, const int64_t* __restrict__ row_ptr,
+                                                         const int32_t* __restrict__ col, const VT* __restrict__ val,
+                                                         const double2* __restrict__ Vc, double2* __restrict__ Vp,
+                                                         KrylovState S, int it) {
+    constexpr int NW = NT / 32;
+    constexpr int SLOTS = 32 / KW;
+    __shared__ double sh[NW * KW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int slot = lane / KW, c = lane % KW;
+    const int k = S.k;
+    const bool mine = slot < SLOTS && c < k;
+    const double bprev = (mine && it > 0) ? S.beta[c] * S.sprev[c] : 0.0;
+    const double scur = mine ? S.scur[c] : 0.0;
+    double apart = 0.0;
+    const int64_t rstep = (int64_t)gridDim.x * NW * SLOTS;
+    for (int64_t rb = ((int64_t)blockIdx.x * NW + warp) * SLOTS; rb < n; rb += rstep) {
+        const int64_t r = rb + slot;
+        const bool live = slot < SLOTS && r < n;
+        const int64_t s = live ? __ldg(row_ptr + r) : 0, e = live ? __ldg(row_ptr + r + 1) : 0;
+        double2 acc;
+        row_times_x_slot<KW, VT, double2>(s, e, col, val, Vc, k, c, c < k, acc);
+        if (live && c < k) {
+            const int64_t o = r * k + c;
+            const double2 vp = Vp[o];
+            double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
+            w.x = w.x + scur * acc.x;
+            w.y = w.y + scur * acc.y;
+            Vp[o] = w;
+            const double2 vc = Vc[o];
+            apart += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
+        }
+    }
+    double tot = 0.0;
+#pragma unroll
+    for (int q = 0; q < SLOTS; ++q) tot += __shfl_sync(0xffffffffu, apart, q * KW + (lane % KW));
+    if (lane < KW) sh[warp * KW + lane] = tot;
+    __syncthreads();
+    for (int i = threadIdx.x; i < KW; i += NT) {
+        double t = 0.0;
+        for (int w = 0; w < NW; ++w) t += sh[w * KW + i];
+        if (i < k) S.part[(int64_t)blockIdx.x * k + i] = t;
+    }
+    __syncthreads();
+    if (arrive_last(S.ticket)) {
+        for (int j = threadIdx.x; j < k; j += NT) {
+            const double a = S.scur[j] * sum_partials(S.part, gridDim.x, k, j);
+            S.alpha[j] = a;
+            if (S.active[j]) S.alpha_out[(int64_t)j * S.maxn + it] = a;
+        }
+        if (threadIdx.x == 0) *S.ticket = 0u;
+    }
+}
+
 // ---- K9a on the tiled layout ------------------------------------------------------------
 // One block per (row tile, 32 columns).  The block walks the pieces of its row tile; for
 // each piece it stages the column tile of V_cur (32 columns, up to EDX_TILE_COLS_MAX rows)
@@ -797,9 +853,33 @@ static int launch_apply_tg(const edx_csr* A, const double2* Vc, double2* Vp, con
     }
 }
 
+template <int KW, class VT>
+static int launch_apply_rs(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+                           const ApplyCfg& cfg, cudaStream_t st) {
+    const VT* v = reinterpret_cast<const VT*>(A->val);
+    if (cfg.threads == 1024)
+        k_lanczos_apply_rs<KW, VT, 1024><<<cfg.gx, 1024, 0, st>>>(A->nrows, A->row_ptr, A->col, v, Vc, Vp, S, it);
+    else
+        k_lanczos_apply_rs<KW, VT, 256><<<cfg.gx, 256, 0, st>>>(A->nrows, A->row_ptr, A->col, v, Vc, Vp, S, it);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}
+
 template <class VT>
 static int apply_v(const edx_csr* A, const double2* Vc, double2* Vp, const KrylovState& S, int it,
                    const ApplyCfg& cfg, cudaStream_t st) {
+    if (cfg.rowslot) {
+        switch (cfg.kw) {
+        case 1: return launch_apply_rs<1, VT>(A, Vc, Vp, S, it, cfg, st);
+        case 2: return launch_apply_rs<2, VT>(A, Vc, Vp, S, it, cfg, st);
+        case 4: return launch_apply_rs<4, VT>(A, Vc, Vp, S, it, cfg, st);
+        case 6: return launch_apply_rs<6, VT>(A, Vc, Vp, S, it, cfg, st);
+        case 8: return launch_apply_rs<8, VT>(A, Vc, Vp, S, it, cfg, st);
+        case 12: return launch_apply_rs<12, VT>(A, Vc, Vp, S, it, cfg, st);
+        case 16: return launch_apply_rs<16, VT>(A, Vc, Vp, S, it, cfg, st);
+        }
+        return fail(EDX_ERR_INVALID, "krylov: one row per slot needs a column group of at most 16");
+    }
     switch (cfg.kw) {
     case 1: return launch_apply<1, 1, VT>(A, Vc, Vp, S, it, cfg, st);
     case 2: return launch_apply<2, 1, VT>(A, Vc, Vp, S, it, cfg, st);
@@ -1078,8 +1158,8 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
                     "edx_krylov: apply_packed does not describe this matrix");
     }
     if (cfg.rowslot)
-        EDX_REQUIRE(packed && !layout && cfg.kw <= 16 && k <= cfg.kw,
-                    "edx_krylov: apply_rowslot needs the packed form and k <= apply_col_group <= 16");
+        EDX_REQUIRE(!layout && cfg.kw <= 16 && k <= cfg.kw,
+                    "edx_krylov: apply_rowslot needs k <= apply_col_group <= 16 (and no tiled layout)");
     const int kw = pow2_kw(k);  // layout of the element-wise recurrence kernels
     const int gy = (k + kw - 1) / kw;
     int gx = num_sms() * 8;

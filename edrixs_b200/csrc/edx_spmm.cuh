@@ -310,6 +310,33 @@ __device__ __forceinline__ void spmv_rows_half(int64_t p0, int64_t pstep, int64_
     }
 }
 
+// Short rows (a transition operator has ~10 entries per row): each slot of the warp owns a
+// row of its own and walks its entries, U at a time, with the slot's KW lanes reading the
+// same entry (a broadcast) and gathering their own columns of X.  No cross-slot reduction.
+template <int KW, class VT, class XT>
+__device__ __forceinline__ void row_times_x_slot(int64_t start, int64_t end, const int32_t* __restrict__ col,
+                                                 const VT* __restrict__ val, const XT* __restrict__ X,
+                                                 int64_t ldx_, int gc, bool colok, typename Acc<VT, XT>::T& acc) {
+    using AT = typename Acc<VT, XT>::T;
+    constexpr int U = 4;
+    acc = zero_c<AT>();
+    for (int64_t base = start; base < end; base += U) {
+        int cc[U];
+        AT vv[U], xs[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool ok = base + u < end;
+            cc[u] = ok ? __ldg(col + base + u) : 0;
+            vv[u] = ok ? to_acc(__ldg(val + base + u), AT()) : zero_c<AT>();
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            xs[u] = (base + u < end && colok) ? to_acc(ldx(X + (int64_t)cc[u] * ldx_ + gc), AT()) : zero_c<AT>();
+#pragma unroll
+        for (int u = 0; u < U; ++u) acc = fma_c(vv[u], xs[u], acc);
+    }
+}
+
 // Streaming loads of packed entry words (read once per product).
 __device__ __forceinline__ uint4 ld_stream4(const uint32_t* p) {
     uint4 v;

@@ -49,6 +49,8 @@ def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None,
     V0 = torch.randn((A.nrows, k), dtype=torch.float64, device=dev, generator=g).to(torch.complex128)
     results = []
     cands = candidates(k)
+    if k <= 16:  # one row per lane group on the CSR too
+        cands += [dict(c, rowslot=1) for c in candidates(k) if c["chunked"] == 0]
     if isinstance(A, device.PackedMatrix):  # no CSR: the packed product in every shape
         packed, cands = A, []
     if packed is not None and not c64:

@@ -320,8 +320,8 @@ typedef struct edx_krylov_opts {
     /* leading dimension of d_v0 (0 = k): the start vectors may be k columns of a wider
      * row-major block */
     int64_t v0_ld;
-    /* with apply_packed and k <= apply_col_group <= 16: each lane group walks a row of its
-     * own (no reduction across the groups of a warp per row) */
+    /* with k <= apply_col_group <= 16 (CSR or packed form): each lane group walks a row of
+     * its own (no reduction across the groups of a warp per row) */
     int apply_rowslot;
 } edx_krylov_opts;
 

@@ -317,3 +317,27 @@ def test_denmat_matches_oracle(cuda, dense_small):
     for c in range(3):
         want = orc.denmat(g["fock_i"], nv, vecs[:, c])
         assert np.abs(got[c] - want).max() < 1e-12
+
+
+@pytest.mark.parametrize("c64", [False, True])
+def test_krylov_csr_rowslot_matches(hn_pair, c64):
+    """One row per lane group on the CSR (apply_rowslot): the same recurrences as the warp-per-
+    row product, complex128 and complex64 matrices."""
+    import torch
+    from edrixs_b200 import device
+    ref, gpu = hn_pair
+    if c64:
+        gpu.to_c64()
+    rng = np.random.default_rng(21)
+    V0 = torch.from_numpy(rng.normal(size=(gpu.nrows, 6)) + 1j * rng.normal(size=(gpu.nrows, 6))).cuda()
+    a = device.krylov(gpu, V0, 25, c64=c64)
+    for shape in (dict(col_group=6, threads=256, blocks_per_sm=4, rowslot=1),
+                  dict(col_group=8, threads=1024, blocks_per_sm=1, rowslot=1)):
+        b = device.krylov(gpu, V0, 25, c64=c64, apply=shape)
+        assert torch.equal(a.neff, b.neff)
+        tol = 1e-6 if c64 else 1e-10
+        assert torch.allclose(a.alpha, b.alpha, rtol=tol, atol=tol)
+        assert torch.allclose(a.beta, b.beta, rtol=tol, atol=tol)
+    if not c64:
+        al, be, nrm, neff = orc.build_krylov(ref, V0[:, 0].cpu().numpy(), 25)
+        assert np.allclose(b.alpha[0].cpu().numpy()[:neff], al, rtol=1e-8, atol=1e-8)

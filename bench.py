@@ -126,8 +126,8 @@ def kernel_case_all(args):
     on H_n (6 columns, with shifts and projections) and H_f (256 columns) on the CSR, packed
     and tiled forms with their builders, two MINRES steps on H_n, the continued fraction
     (768 pole sets x 2000 points), the density matrix, the packed SpMM (narrow and wide
-    forms), the Gram-Schmidt passes of the eigensolver and 16 Lanczos steps with streamed
-    projections."""
+    forms), the Gram-Schmidt and CholeskyQR passes of the eigensolver, the few-column Lanczos
+    products with one row per lane group, and 16 Lanczos steps with streamed projections."""
     import torch
     from edrixs_b200 import device
     m, t = workload_terms(args.nbath, args.nelec)
@@ -176,6 +176,11 @@ def kernel_case_all(args):
     Wb = crand(Hn.nrows, 3)
     C = device.gs_dot(B, 45, Wb)
     device.gs_update(B, 45, Wb, C)
+    G = device.gs_gram(Wb)
+    device.gs_rmul(Wb, torch.linalg.inv(G))
+    # the few-column Lanczos products with one row per lane group, packed and CSR
+    device.krylov(Hn, V, 2, apply=dict(col_group=6, threads=256, blocks_per_sm=4, rowslot=1, packed=Pn))
+    device.krylov(Hn, V, 2, apply=dict(col_group=6, threads=256, blocks_per_sm=4, rowslot=1))
     coef = crand(24, 16)
     acc = torch.zeros((Dout.nrows, 24), dtype=torch.complex128, device="cuda")
     device.krylov(Hn, seeds, 16, proj=[Dout], apply=dict(packed=Pn),

@@ -156,6 +156,8 @@ def kernel_case_all(args):
     W = crand(Hf.nrows, 256)
     device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1))
     device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1, packed=Pf))
+    device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=4, threads=1024, blocks_per_sm=2, packed=Pf))
+    device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=256, blocks_per_sm=4, packed=Pf))
     L = device.tiles_for(Hf, bi)
     device.krylov(Hf, W, 2, apply=dict(layout=L))
     device.minres(Hn, x1, 1e-300, 2, alpha=-1.0, sigma=40 + 0.6j)
@@ -188,6 +190,17 @@ def kernel_case_all(args):
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": "all", "nnz_Hn": Hn.nnz, "nnz_Hf": Hf.nnz, "nnz_Din": Din.nnz,
                       "nnz_Dout": Dout.nnz}))
+
+
+# DRAM bytes (read + write) of one H_f Lanczos product over 256 of the 768 columns, from the
+# `--kernel-case all` ncu capture (profiles/all_kernels_dram.md), per launch shape
+# (packed, columns per group, tiles, threads, blocks per SM, chunked)
+HF_DRAM_256 = {
+    (False, 32, 2, 1024, 1, 0): 5.835e9,
+    (True, 32, 2, 1024, 1, 0): 5.111e9,
+    (True, 32, 4, 1024, 2, 0): 7.834e9,
+    (True, 32, 2, 256, 4, 0): 5.136e9,
+}
 
 
 def load_peaks():
@@ -557,10 +570,10 @@ def run_ours(args):
     # DRAM bytes per launch from one ncu capture of the same kernel and launch shape on 256 of
     # the 768 columns (the kernel case above), scaled by the number of 64-column sweeps
     cfg = tuned.get("hf_k768") or {}
-    if (not st.get("hf_tiled") and not st.get("hf_packed") and not args.c64 and st["k_hf"] == 768
-            and cfg.get("col_group") == 32
-            and cfg.get("tiles") == 2 and cfg.get("chunked") == 0 and cfg.get("threads") == 1024):
-        r_hf["traffic"] = 3 * 5.725e9
+    shape = (bool(st.get("hf_packed")), cfg.get("col_group"), cfg.get("tiles"), cfg.get("threads"),
+             cfg.get("blocks_per_sm"), cfg.get("chunked"))
+    if not st.get("hf_tiled") and not args.c64 and st["k_hf"] == 768 and shape in HF_DRAM_256:
+        r_hf["traffic"] = 3 * HF_DRAM_256[shape]
         r_hf["traffic_source"] = "ncu dram__bytes_read+write on 256 columns (same shape) x 3"
     r_hn = roof(st["hn_nnz"], st["hn_rows"], st["k_hn"], st["hn_apply_ms"], st["hn_iterations"], args.c64,
                 P.packed.get("hn") if st.get("hn_packed") else None)

@@ -716,7 +716,9 @@ __global__ void k_start(int64_t n, int k, const double2* __restrict__ V0, int64_
         const int c = (int)(e - r * k);
         double2 v = V0[r * ld0 + c];
         const double d = s[c];
-        Vc[e] = make_double2(v.x / d, v.y / d);
+        // a zero start vector stays zero (its recurrence stops after one step with norm 0),
+        // where v / |v| would fill the column with NaN
+        Vc[e] = d > 0.0 ? make_double2(v.x / d, v.y / d) : make_double2(0.0, 0.0);
         Vp[e] = make_double2(0.0, 0.0);
     }
 }

@@ -341,3 +341,23 @@ def test_krylov_csr_rowslot_matches(hn_pair, c64):
     if not c64:
         al, be, nrm, neff = orc.build_krylov(ref, V0[:, 0].cpu().numpy(), 25)
         assert np.allclose(b.alpha[0].cpu().numpy()[:neff], al, rtol=1e-8, atol=1e-8)
+
+
+def test_krylov_zero_start_column(hn_pair):
+    """A zero start vector among others: its recurrence stops after one step with norm 0 and
+    finite coefficients (so it adds nothing to a spectrum), and the other columns are the
+    same as without it."""
+    import torch
+    from edrixs_b200 import device
+    ref, gpu = hn_pair
+    rng = np.random.default_rng(31)
+    V = rng.normal(size=(gpu.nrows, 3)) + 1j * rng.normal(size=(gpu.nrows, 3))
+    V[:, 1] = 0
+    r = device.krylov(gpu, torch.from_numpy(V).cuda(), 20)
+    assert r.norm[1].item() == 0.0 and r.neff[1].item() == 1
+    assert torch.isfinite(r.alpha).all() and torch.isfinite(r.beta).all()
+    s = device.krylov(gpu, torch.from_numpy(V[:, [0, 2]].copy()).cuda(), 20)
+    assert torch.allclose(r.alpha[[0, 2]], s.alpha, rtol=1e-12, atol=1e-12)
+    spec = device.cf_spectrum(r.neff, r.alpha, r.beta, np.zeros(3), r.norm.cpu().numpy(), np.ones(3),
+                              np.linspace(-5, 5, 50), 0.3, per_set=True)
+    assert torch.isfinite(spec).all() and spec[1].abs().max().item() == 0.0

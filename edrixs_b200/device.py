@@ -427,7 +427,8 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
     if apply and apply.get("packed") is not None and "rowslot" not in apply and kcols <= 16 \
             and "col_group" not in apply:
         # a few columns on the packed form: one row per lane group, the measured best shape
-        apply = dict({"threads": 256, "blocks_per_sm": 4}, **apply, rowslot=1)
+        th = int(apply.get("threads", 256))
+        apply = dict({"threads": th, "blocks_per_sm": 4 if th == 256 else 1}, **apply, rowslot=1)
     V0 = V0.reshape(V0.shape[0], -1)
     if (V0.shape[1] > 1 and V0.stride(1) != 1) or V0.stride(0) < V0.shape[1]:
         V0 = V0.contiguous()

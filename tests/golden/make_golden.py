@@ -19,6 +19,10 @@ What it writes (all small):
   siam_callers/      the exact files ed_siam_fort (do_ed=2), xas_siam_fort and rixs_siam_fort
                      write before calling the solver (captured with a recording stand-in for
                      edrixs.fedrixs).
+  kh_1v1c/           a d8 ion with a 2p core: XAS and RIXS spectra from the reference's
+                     pure-Python Kramers-Heisenberg solvers (xas_1v1c_py, rixs_1v1c_py on
+                     ed_1v1c_py eigenstates) and the input files its Fortran-path callers write
+                     for the same ion.
 """
 import hashlib
 import json
@@ -259,6 +263,88 @@ def siam_callers(ed, out_dir):
     del hopping
 
 
+def kh_1v1c(ed, out_dir):
+    """An independent answer for the XAS and RIXS drivers: a d8 ion with a 2p core (45
+    initial, 60 intermediate states), solved by the reference's pure-Python path --
+    ed_1v1c_py (dense eigenproblems), xas_1v1c_py and rixs_1v1c_py (Kramers-Heisenberg sums
+    over all eigenstates, edrixs/solvers.py:28-571) -- and the input files that the
+    reference's Fortran-path callers ed_1v1c_fort / xas_1v1c_fort / rixs_1v1c_fort write for
+    the same ion (captured with a recording stand-in for edrixs.fedrixs).  A Lanczos run to
+    the full dimension reproduces the Kramers-Heisenberg spectra, so the oracle drivers on
+    those files must give them."""
+    rng = np.random.default_rng(17)
+    a = rng.normal(scale=0.15, size=(10, 10)) + 1j * rng.normal(scale=0.15, size=(10, 10))
+    cf = a + a.conj().T  # generic crystal field: a non-degenerate ground state
+    kw = dict(shell_level=(0.0, -100.0), v_soc=(0.08, 0.1), c_soc=11.0, v_noccu=8,
+              slater=([8.0, 10.0, 6.2], [8.0, 10.0, 6.2, 7.0, 6.0, 4.5, 2.6]), v_cfmat=cf)
+    eval_i, eval_n, trans_op = ed.ed_1v1c_py(("d", "p"), **kw)
+    edge = float(eval_n[0] - eval_i[0])
+    ominc = edge + np.linspace(-2.0, 8.0, 41)
+    eloss = np.linspace(-0.5, 6.0, 66)
+    xas_pol = [("linear", 0.0), ("left", 0.0)]
+    rixs_pol = [("linear", 0.0, "linear", np.pi / 2), ("linear", np.pi / 2, "linear", 0.0)]
+    geo = dict(thin=0.6, phi=0.3)
+    T = 10.0
+    xas = ed.xas_1v1c_py(eval_i, eval_n, trans_op, ominc, gamma_c=0.3, pol_type=xas_pol, gs_list=[0],
+                         temperature=T, **geo)
+    rixs = ed.rixs_1v1c_py(eval_i, eval_n, trans_op, ominc[::8], eloss, gamma_c=0.6, gamma_f=0.1, thout=1.1,
+                           pol_type=rixs_pol, gs_list=[0], temperature=T, **geo)
+    calls = {"n": 0}
+
+    def recorder(kind):
+        def fsolver(comm, my_id, num_procs):
+            calls["n"] += 1
+            d = os.path.join(out_dir, f"{kind}_{calls['n']:02d}")
+            os.makedirs(d, exist_ok=True)
+            for fn in os.listdir("."):
+                if fn.endswith(".in"):
+                    shutil.copy(fn, os.path.join(d, fn))
+            if kind in ("xas", "rixs"):  # minimal outputs so that the caller can go on
+                with open(f"{kind}_poles.1", "w") as f:
+                    f.write("#number_of_poles:            1\n#enegry:                  0.0\n"
+                            "#normalization:           1.0\n    1      0.0      0.0\n")
+        return fsolver
+
+    mod = types.ModuleType("edrixs.fedrixs")
+    mod.ed_fsolver, mod.xas_fsolver, mod.rixs_fsolver = recorder("ed"), recorder("xas"), recorder("rixs")
+    sys.modules["edrixs.fedrixs"] = mod
+    if os.path.isdir(out_dir):
+        shutil.rmtree(out_dir)
+    os.makedirs(out_dir)
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as td:
+        os.chdir(td)
+        try:
+            comm = FakeComm()
+            ed.ed_1v1c_fort(comm, ("d", "p"), do_ed=False, ed_solver=0, neval=3, nvector=1, min_ndim=1000, **kw)
+            d = os.path.join(out_dir, "ed_00")  # do_ed=False: the files only, no solver call
+            os.makedirs(d)
+            for fn in os.listdir("."):
+                if fn.endswith(".in"):
+                    shutil.copy(fn, os.path.join(d, fn))
+            ed.xas_1v1c_fort(comm, ("d", "p"), ominc, gamma_c=0.3, v_noccu=8, pol_type=xas_pol, num_gs=1,
+                             nkryl=200, temperature=T, **geo)
+            ed.rixs_1v1c_fort(comm, ("d", "p"), ominc[::8], eloss, gamma_c=0.6, gamma_f=0.1, v_noccu=8, thout=1.1,
+                              pol_type=rixs_pol, num_gs=1, nkryl=200, linsys_max=1000, linsys_tol=1e-13,
+                              temperature=T, **geo)
+        finally:
+            os.chdir(cwd)
+    # keep one copy of the files every call shares (Hamiltonian terms, initial basis)
+    base = os.path.join(out_dir, "ed_00")
+    for d in sorted(os.listdir(out_dir)):
+        if d == "ed_00":
+            continue
+        for fn in os.listdir(os.path.join(out_dir, d)):
+            p = os.path.join(out_dir, d, fn)
+            q = os.path.join(base, fn)
+            if os.path.exists(q) and open(p, "rb").read() == open(q, "rb").read():
+                os.remove(p)
+    np.savez(os.path.join(out_dir, "kh_spectra.npz"), eval_i=eval_i, eval_n=eval_n, ominc=ominc,
+             ominc_rixs=ominc[::8], eloss=eloss, xas=xas, rixs=rixs, gamma_c_xas=0.3, gamma_c_rixs=0.6,
+             gamma_f=0.1, temperature=T)
+    return sorted(os.listdir(out_dir))
+
+
 def main(ref):
     ed = import_reference(ref)
     known_answer(ed, os.path.join(HERE, "known_answer"))
@@ -266,6 +352,7 @@ def main(ref):
     fock_digests(ed, os.path.join(HERE, "fock_digests.json"))
     spectra(ed, os.path.join(HERE, "spectra.npz"))
     siam_callers(ed, os.path.join(HERE, "siam_callers"))
+    print("kh_1v1c", kh_1v1c(ed, os.path.join(HERE, "kh_1v1c")))
     print("golden fixtures written to", HERE)
 
 

@@ -19,6 +19,8 @@ What it writes (all small):
   siam_callers/      the exact files ed_siam_fort (do_ed=2), xas_siam_fort and rixs_siam_fort
                      write before calling the solver (captured with a recording stand-in for
                      edrixs.fedrixs).
+  denmat.npz         <c+_i c_j> of the two lowest eigenstates of the dense_small H_i, every
+                     operator built by manybody_operator.two_fermion.
   kh_1v1c/           a d8 ion with a 2p core: XAS and RIXS spectra from the reference's
                      pure-Python Kramers-Heisenberg solvers (xas_1v1c_py, rixs_1v1c_py on
                      ed_1v1c_py eigenstates) and the input files its Fortran-path callers write
@@ -345,6 +347,30 @@ def kh_1v1c(ed, out_dir):
     return sorted(os.listdir(out_dir))
 
 
+def denmat_golden(ed, dense_path, out_path):
+    """<c+_i c_j> of the ground state and of the first excited state of the dense_small H_i,
+    each operator built by the reference's manybody_operator.two_fermion on the same basis
+    (an independent route to what src/ed_driver.f90:194-248 computes)."""
+    with np.load(dense_path) as z:
+        d = {k: z[k] for k in z.files}
+    nv = int(d["nv"])
+    n = int(d["H_i_shape"][0])
+    H = np.zeros((n, n), dtype=complex)
+    H[d["H_i_row"], d["H_i_col"]] = d["H_i_val"]
+    e, v = np.linalg.eigh(H)
+    basis = [bits(int(st), nv) for st in d["fock_i"]]
+    rho = np.zeros((2, nv, nv), dtype=complex)
+    for i in range(nv):
+        for j in range(nv):
+            E = np.zeros((nv, nv), dtype=complex)
+            E[i, j] = 1.0
+            M = ed.two_fermion(E, basis)
+            for k in range(2):
+                rho[k, i, j] = v[:, k].conj() @ M @ v[:, k]
+    np.savez(out_path, eigvals=e[:3], rho=rho)
+    return float(e[1] - e[0]), float(e[2] - e[1])
+
+
 def main(ref):
     ed = import_reference(ref)
     known_answer(ed, os.path.join(HERE, "known_answer"))
@@ -353,6 +379,7 @@ def main(ref):
     spectra(ed, os.path.join(HERE, "spectra.npz"))
     siam_callers(ed, os.path.join(HERE, "siam_callers"))
     print("kh_1v1c", kh_1v1c(ed, os.path.join(HERE, "kh_1v1c")))
+    print("denmat", denmat_golden(ed, os.path.join(HERE, "dense_small.npz"), os.path.join(HERE, "denmat.npz")))
     print("golden fixtures written to", HERE)
 
 

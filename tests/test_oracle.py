@@ -154,3 +154,22 @@ def test_denmat_oracle_trace(dense_small):
     dm = orc.denmat(g["fock_i"], int(g["nv"]), v[:, 0])
     assert abs(np.trace(dm).real - int(g["nelec"])) < 1e-10
     assert np.allclose(dm, dm.conj().T, atol=1e-10)
+
+
+def test_denmat_matches_reference_two_fermion(dense_small, golden_dir):
+    """<c+_i c_j> of the two lowest eigenstates of the dense_small H_i: the oracle's restatement
+    of ed_driver.f90:194-248 against every operator built by the reference's
+    manybody_operator.two_fermion (tests/golden/denmat.npz).  Eigenvector phases cancel; the
+    reference skips rows with |v_a| < 1e-10 in the off-diagonals, so 1e-9 absolute."""
+    g = dense_small
+    nv = int(g["nv"])
+    csr = orc.build_csr("ham_i", g["fock_i"], (g["hop_i_idx"], g["hop_i_val"]), (g["coul_i_idx"], g["coul_i_val"]),
+                        num_val_orbs=nv)
+    e, v = np.linalg.eigh(csr.dense())
+    with np.load(os.path.join(golden_dir, "denmat.npz")) as z:
+        rho, ev = z["rho"], z["eigvals"]
+    assert np.allclose(e[:3], ev, atol=1e-12)
+    for k in range(2):
+        got = orc.denmat(g["fock_i"], nv, v[:, k])
+        assert np.allclose(got, rho[k], atol=1e-9, rtol=0)
+        assert abs(np.trace(got).real - int(g["nelec"])) < 1e-9

@@ -106,6 +106,23 @@ def rixs(directory):
     return out
 
 
+def opavg(directory):
+    """-> (eigvals, <v|O|v>) per eigvec.N, N = 1..num_gs (src/opavg_driver.f90:62-112): O is
+    built from hopping_i.in / coulomb_i.in on fock_i.in as build_ham_i builds a Hamiltonian,
+    then dot_product(v, O v) (:103-106)."""
+    p = lambda f: os.path.join(directory, f)  # noqa: E731
+    cfg = _cfg(p("config.in"))
+    fock = orc.read_fock(p("fock_i.in"))
+    O = orc.build_csr("ham_i", fock, orc.read_terms(p("hopping_i.in"), 2), orc.read_terms(p("coulomb_i.in"), 4),
+                      num_val_orbs=cfg["num_val_orbs"])
+    ev, avg = [], []
+    for igs in range(1, cfg["num_gs"] + 1):
+        e, v = read_eigvec(p(f"eigvec.{igs}"))
+        ev.append(e)
+        avg.append(np.vdot(v, orc.matvec(O, v)))
+    return np.array(ev), np.array(avg)
+
+
 def rixs_in_memory(terms, nv, nelec, gs_e, gs_v, din_terms, dout_terms, omegas, gamma_c, eloss, gamma_f, nkryl,
                    tol, maxit, temperature):
     """The reference's loop (solvers.py:2651-2702) for every omega x pol pair x ground state;

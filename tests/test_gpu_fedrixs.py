@@ -188,3 +188,19 @@ def test_rixs_streamed_projections_match_stored(cuda, window):
                           atol=1e-10)
     assert rel_linf(b.spectra, a.spectra) < 1e-8
     assert rel_linf(b.spectra, ref) < 1e-6
+
+
+def test_opavg_drop_in(cuda, dense_small, golden_dir, workdir):
+    """opavg_fsolver (src/opavg_driver.f90) on the d-electron number operator: opavg.dat equals
+    the oracle's <v|O|v> and the reference two_fermion density matrices' d-orbital traces."""
+    import test_oracle
+    from edrixs_b200 import fedrixs
+    from oracle import drivers as odrv
+    e, want = test_oracle._opavg_case(dense_small, golden_dir, str(workdir))
+    ev, ref = odrv.opavg(str(workdir))
+    fedrixs.opavg_fsolver(0, 0, 1)
+    data = np.loadtxt("opavg.dat", ndmin=2)
+    assert data.shape == (2, 4)
+    assert np.allclose(data[:, 1], e, atol=1e-10)
+    assert np.allclose(data[:, 2] + 1j * data[:, 3], ref, atol=1e-10)
+    assert np.allclose(data[:, 2], want.real, atol=1e-10)

@@ -173,3 +173,47 @@ def test_denmat_matches_reference_two_fermion(dense_small, golden_dir):
         got = orc.denmat(g["fock_i"], nv, v[:, k])
         assert np.allclose(got, rho[k], atol=1e-9, rtol=0)
         assert abs(np.trace(got).real - int(g["nelec"])) < 1e-9
+
+
+def _opavg_case(dense_small, golden_dir, d):
+    """A working directory for opavg: the d-electron number operator (orbitals 1..10) as
+    hopping_i.in, no Coulomb terms, the dense_small basis and its two lowest eigenvectors.
+    Returns the expected <N_d> from the reference two_fermion density matrices."""
+    from edrixs_b200 import io as edxio
+    g = dense_small
+    nv = int(g["nv"])
+    csr = orc.build_csr("ham_i", g["fock_i"], (g["hop_i_idx"], g["hop_i_val"]), (g["coul_i_idx"], g["coul_i_val"]),
+                        num_val_orbs=nv)
+    e, v = np.linalg.eigh(csr.dense())
+    E = np.zeros((nv, nv), dtype=complex)
+    E[:10, :10] = np.eye(10)
+    edxio.write_emat(E, os.path.join(d, "hopping_i.in"))
+    edxio.write_umat(np.zeros((nv,) * 4, dtype=complex), os.path.join(d, "coulomb_i.in"))
+    edxio.write_fock(os.path.join(d, "fock_i.in"), g["fock_i"])
+    edxio.write_config(d, num_val_orbs=nv, num_core_orbs=0, num_gs=2)
+    for k in range(2):
+        edxio.write_eigvec(os.path.join(d, f"eigvec.{k + 1}"), e[k], v[:, k])
+    with np.load(os.path.join(golden_dir, "denmat.npz")) as z:
+        rho = z["rho"]
+    return e[:2], np.array([np.trace(rho[k][:10, :10]) for k in range(2)])
+
+
+def test_opavg_matches_reference_two_fermion(dense_small, golden_dir, tmp_path):
+    """opavg_driver.f90 restated: <v|N_d|v> of two eigenvectors equals the trace over the d
+    orbitals of the reference's two_fermion density matrices."""
+    from oracle import drivers as odrv
+    e, want = _opavg_case(dense_small, golden_dir, str(tmp_path))
+    ev, got = odrv.opavg(str(tmp_path))
+    assert np.allclose(ev, e, atol=1e-14)
+    assert np.allclose(got, want, atol=1e-12)
+    assert np.all(np.abs(got.imag) < 1e-13)
+
+
+def test_opavg_file_format(tmp_path):
+    """write_opavg = src/io.f90:638-659: i5, then eigenvalue, Re and Im as f20.10."""
+    from edrixs_b200 import io as edxio
+    p = str(tmp_path / "opavg.dat")
+    edxio.write_opavg(p, [-12.5, 3.0], [complex(2.25, -0.0), -1.0 + 1e-12j])  # negative zero keeps its sign
+    lines = open(p).read().splitlines()
+    assert lines[0] == "    1" + "{:20.10f}".format(-12.5) + "{:20.10f}".format(2.25) + "{:20.10f}".format(-0.0)
+    assert len(lines[1]) == 65 and lines[1].startswith("    2")

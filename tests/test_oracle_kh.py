@@ -69,3 +69,23 @@ def test_rixs_matches_kramers_heisenberg(golden, tmp_path):
         runs = odrv.rixs(_workdir(tmp_path, name, gs))
         spec = orc.spectra_from_poles(_poles(runs), g["eloss"], float(g["gamma_f"]), float(g["temperature"]))
         assert rel(spec, g["rixs"][iw, :, ip]) < 1e-10, (name, rel(spec, g["rixs"][iw, :, ip]))
+
+
+def test_spectra_of_both_hamiltonians_match_reference():
+    """All 45 initial and 60 intermediate eigenvalues of the oracle's H_i and H_n, built from
+    the files the reference's callers wrote, equal those of ed_1v1c_py (which builds both
+    Hamiltonians with its own two_fermion / four_fermion and diagonalises them densely)."""
+    with np.load(os.path.join(KH, "kh_spectra.npz")) as z:
+        eval_i, eval_n = z["eval_i"], z["eval_n"]
+    base, xd = os.path.join(KH, "ed_00"), os.path.join(KH, "xas_01")
+    cfg = odrv._cfg(os.path.join(xd, "config.in"))
+    nv, nc = cfg["num_val_orbs"], cfg["num_core_orbs"]
+    Hi = orc.build_csr("ham_i", orc.read_fock(os.path.join(base, "fock_i.in")),
+                       orc.read_terms(os.path.join(base, "hopping_i.in"), 2),
+                       orc.read_terms(os.path.join(base, "coulomb_i.in"), 4), num_val_orbs=nv)
+    Hn = orc.build_csr("ham_n", orc.read_fock(os.path.join(xd, "fock_n.in")),
+                       orc.read_terms(os.path.join(base, "hopping_n.in"), 2),
+                       orc.read_terms(os.path.join(base, "coulomb_n.in"), 4), num_val_orbs=nv, num_core_orbs=nc)
+    assert Hi.nrows == len(eval_i) and Hn.nrows == len(eval_n)
+    assert np.allclose(np.linalg.eigvalsh(Hi.dense()), eval_i, atol=1e-10)
+    assert np.allclose(np.linalg.eigvalsh(Hn.dense()), eval_n, atol=1e-10)

@@ -24,7 +24,7 @@ What it writes (all small):
   kh_1v1c/           a d8 ion with a 2p core: XAS and RIXS spectra from the reference's
                      pure-Python Kramers-Heisenberg solvers (xas_1v1c_py, rixs_1v1c_py on
                      ed_1v1c_py eigenstates) and the input files its Fortran-path callers write
-                     for the same ion.
+                     for the same ion; also a thermal case (3 ground states at 3000 K).
 """
 import hashlib
 import json
@@ -291,20 +291,30 @@ def kh_1v1c(ed, out_dir):
                          temperature=T, **geo)
     rixs = ed.rixs_1v1c_py(eval_i, eval_n, trans_op, ominc[::8], eloss, gamma_c=0.6, gamma_f=0.1, thout=1.1,
                            pol_type=rixs_pol, gs_list=[0], temperature=T, **geo)
+    # a thermal case: three ground states with Boltzmann weights at 3000 K
+    Th = 3000.0
+    xas_t = ed.xas_1v1c_py(eval_i, eval_n, trans_op, ominc, gamma_c=0.3, pol_type=xas_pol[:1], gs_list=[0, 1, 2],
+                           temperature=Th, **geo)
+    rixs_t = ed.rixs_1v1c_py(eval_i, eval_n, trans_op, ominc[8:17:8], eloss, gamma_c=0.6, gamma_f=0.1, thout=1.1,
+                             pol_type=rixs_pol[:1], gs_list=[0, 1, 2], temperature=Th, **geo)
     calls = {"n": 0}
 
     def recorder(kind):
         def fsolver(comm, my_id, num_procs):
             calls["n"] += 1
-            d = os.path.join(out_dir, f"{kind}_{calls['n']:02d}")
+            tag = "t" if "thermal" in calls else ""
+            d = os.path.join(out_dir, f"{kind}{tag}_{calls['n']:02d}")
             os.makedirs(d, exist_ok=True)
             for fn in os.listdir("."):
                 if fn.endswith(".in"):
                     shutil.copy(fn, os.path.join(d, fn))
             if kind in ("xas", "rixs"):  # minimal outputs so that the caller can go on
-                with open(f"{kind}_poles.1", "w") as f:
-                    f.write("#number_of_poles:            1\n#enegry:                  0.0\n"
-                            "#normalization:           1.0\n    1      0.0      0.0\n")
+                import re
+                ngs = int(re.search(r"num_gs=(\d+)", open("config.in").read()).group(1))
+                for g in range(ngs):
+                    with open(f"{kind}_poles.{g + 1}", "w") as f:
+                        f.write("#number_of_poles:            1\n#enegry:                  0.0\n"
+                                "#normalization:           1.0\n    1      0.0      0.0\n")
         return fsolver
 
     mod = types.ModuleType("edrixs.fedrixs")
@@ -329,6 +339,12 @@ def kh_1v1c(ed, out_dir):
             ed.rixs_1v1c_fort(comm, ("d", "p"), ominc[::8], eloss, gamma_c=0.6, gamma_f=0.1, v_noccu=8, thout=1.1,
                               pol_type=rixs_pol, num_gs=1, nkryl=200, linsys_max=1000, linsys_tol=1e-13,
                               temperature=T, **geo)
+            calls["thermal"] = calls["n"]  # calls after this one are the thermal case
+            ed.xas_1v1c_fort(comm, ("d", "p"), ominc, gamma_c=0.3, v_noccu=8, pol_type=xas_pol[:1], num_gs=3,
+                             nkryl=200, temperature=Th, **geo)
+            ed.rixs_1v1c_fort(comm, ("d", "p"), ominc[8:17:8], eloss, gamma_c=0.6, gamma_f=0.1, v_noccu=8,
+                              thout=1.1, pol_type=rixs_pol[:1], num_gs=3, nkryl=200, linsys_max=1000,
+                              linsys_tol=1e-13, temperature=Th, **geo)
         finally:
             os.chdir(cwd)
     # keep one copy of the files every call shares (Hamiltonian terms, initial basis)
@@ -343,7 +359,8 @@ def kh_1v1c(ed, out_dir):
                 os.remove(p)
     np.savez(os.path.join(out_dir, "kh_spectra.npz"), eval_i=eval_i, eval_n=eval_n, ominc=ominc,
              ominc_rixs=ominc[::8], eloss=eloss, xas=xas, rixs=rixs, gamma_c_xas=0.3, gamma_c_rixs=0.6,
-             gamma_f=0.1, temperature=T)
+             gamma_f=0.1, temperature=T, xas_thermal=xas_t, rixs_thermal=rixs_t, ominc_rixs_thermal=ominc[8:17:8],
+             temperature_thermal=Th)
     return sorted(os.listdir(out_dir))
 
 

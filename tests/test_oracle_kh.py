@@ -89,3 +89,37 @@ def test_spectra_of_both_hamiltonians_match_reference():
     assert Hi.nrows == len(eval_i) and Hn.nrows == len(eval_n)
     assert np.allclose(np.linalg.eigvalsh(Hi.dense()), eval_i, atol=1e-10)
     assert np.allclose(np.linalg.eigvalsh(Hn.dense()), eval_n, atol=1e-10)
+
+
+def test_thermal_xas_rixs_match_kramers_heisenberg(tmp_path):
+    """Three ground states with Boltzmann weights at 3000 K (num_gs = 3: eigvec.1..3, one
+    pole set each, summed by get_spectra_from_poles) against gs_list = [0, 1, 2] of the
+    reference's Kramers-Heisenberg solvers."""
+    from edrixs_b200 import io as edxio
+    with np.load(os.path.join(KH, "kh_spectra.npz")) as z:
+        g = {k: z[k] for k in z.files}
+    base = os.path.join(KH, "ed_00")
+    Hi = orc.build_csr("ham_i", orc.read_fock(os.path.join(base, "fock_i.in")),
+                       orc.read_terms(os.path.join(base, "hopping_i.in"), 2),
+                       orc.read_terms(os.path.join(base, "coulomb_i.in"), 4), num_val_orbs=10)
+    e, v = np.linalg.eigh(Hi.dense())
+    T = float(g["temperature_thermal"])
+
+    def workdir(name):
+        d = tmp_path / name
+        d.mkdir()
+        for src in (base, os.path.join(KH, name)):
+            for fn in os.listdir(src):
+                shutil.copy(os.path.join(src, fn), d / fn)
+        for k in range(3):
+            edxio.write_eigvec(str(d / f"eigvec.{k + 1}"), e[k], v[:, k])
+        return str(d)
+
+    runs = odrv.xas(workdir("xast_15"))
+    assert len(runs) == 3
+    spec = orc.spectra_from_poles(_poles(runs), g["ominc"], float(g["gamma_c_xas"]), T)
+    assert rel(spec, g["xas_thermal"][:, 0]) < 1e-10
+    for iw, name in enumerate(["rixst_16", "rixst_17"]):
+        runs = odrv.rixs(workdir(name))
+        spec = orc.spectra_from_poles(_poles(runs), g["eloss"], float(g["gamma_f"]), T)
+        assert rel(spec, g["rixs_thermal"][iw, :, 0]) < 1e-10

@@ -41,3 +41,56 @@ def test_coalesce_key_groups_compatible_requests():
     x2 = Request("xas", m, ngs=2, eloss=el[:10], pols=(1,), nkryl=200)
     assert coalesce_key(x1) == coalesce_key(x2) != coalesce_key(a)
     assert coalesce_key(Request("ed", m)) is None
+
+
+def test_scheduler_groups_waiting_requests_when_a_worker_frees():
+    """The scheduler (no GPU: a fake worker takes the jobs) hands a request to a worker only
+    when one is free, and takes every waiting request with the same coalesce_key along."""
+    import threading
+    import time
+    from edrixs_b200.serve import ModelSpec, Request, Server
+    srv = Server(hbm_budget=1e12, workers=1)
+    groups = []
+    release = threading.Event()
+
+    def fake_worker():
+        while True:
+            job = srv.jobs.get()
+            if job is None:
+                return
+            group, res, need = job
+            groups.append([r.id for r, _ in group])
+            release.wait(5)
+            with srv.cv:
+                res.busy -= 1
+                srv.inflight_bytes -= need
+                srv.free_workers += 1
+                srv.cv.notify_all()
+
+    sched = threading.Thread(target=srv._schedule, daemon=True)
+    worker = threading.Thread(target=fake_worker, daemon=True)
+    sched.start()
+    worker.start()
+    m, m2 = ModelSpec(4, 7, 1), ModelSpec(4, 7, 2)
+    el = np.linspace(-0.5, 12.0, 100)
+    first = Request("ed", m2)
+    srv.submit(first)
+    time.sleep(0.3)  # the one worker now holds the ED job
+    a = Request("rixs", m, ngs=1, omegas=np.array([1.0]), eloss=el, pols=(0,))
+    x = Request("xas", m, ngs=1, eloss=el, pols=(0,))
+    b = Request("rixs", m, ngs=2, omegas=np.array([2.0]), eloss=el, pols=(1,))
+    c = Request("rixs", m2, ngs=1, omegas=np.array([2.0]), eloss=el, pols=(1,))
+    for r in (a, x, b, c):
+        srv.submit(r)
+    time.sleep(0.3)
+    assert groups == [[first.id]]  # nothing else dispatched while the worker is busy
+    release.set()
+    deadline = time.time() + 5
+    while len(groups) < 4 and time.time() < deadline:
+        time.sleep(0.05)
+    with srv.cv:
+        srv.stop_flag = True
+        srv.cv.notify_all()
+    srv.jobs.put(None)
+    assert groups[1] == [a.id, b.id]  # same Hamiltonian and settings: one solve
+    assert sorted(map(tuple, groups[2:])) == sorted([(x.id,), (c.id,)])

@@ -281,3 +281,82 @@ def ed_eigs(csr, nev, dense_below=3000, tol=1e-13):
     e, v = sla.eigsh(csr.to_scipy(), k=nev, which="SA", tol=tol, ncv=max(2 * nev + 20, 40))
     order = np.argsort(e)
     return e[order], v[:, order]
+
+
+def _tridiag_eigs(alpha, beta):
+    """krylov_eigs (src/lanczos.f90:169-206): dsteqr('I') on the i x i tridiagonal matrix.
+    LAPACK's dstev with vectors runs the same implicit QL/QR (dsteqr)."""
+    from scipy.linalg import lapack
+    d, z, info = lapack.dstev(np.asarray(alpha, dtype=np.float64), np.asarray(beta, dtype=np.float64),
+                              compute_v=1)
+    if info != 0:
+        raise RuntimeError(f"dstev info {info}")
+    return d, z
+
+
+def lanczos_eigs(csr, nev, max_niter, eval_tol, nvec=1, seed=0):
+    """diag_ham_lanczos (src/lanczos.f90:6-167), the ed_solver = 1 path of ed_driver.f90:154-158.
+
+    Plain Lanczos without reorthogonalisation, step for step:
+    * start vector: uniform reals in [-0.5, 0.5), zero imaginary part, normalised
+      (:60-70). The reference calls random_seed() without arguments, so its start vector is
+      processor-dependent; here it is numpy's default generator with `seed`.
+    * step i: w = H v_i - beta_{i-1} v_{i-1}; alpha_i = Re<v_i, w> (:76-88).
+    * every 10th step and at max_niter: eigenvalues of T_i (dsteqr); once i >= nev, stop when
+      |lambda_nev(T_i) - lambda_nev(previous check)| < eval_tol (:89-110). The previous check
+      starts at 0.
+    * w -= alpha_i v_i; beta_i = |w|; stop when beta_i < 1e-10 (:111-131).
+    * eigenvectors: the recurrence is run again from the stored start vector and
+      sum_i z_ij v_i accumulated over the nkrylov steps (:133-157). When max_niter passes
+      without convergence nkrylov stays 0 and the eigenvectors are zero, as in the reference.
+    Where T_i is smaller than nev, the missing eigenvalues read the zeroed work array and are 0.
+    Returns (eval[nev], evec[n, nvec], nkrylov).
+    """
+    n = csr.nrows
+    rng = np.random.default_rng(seed)
+    v1 = (rng.random(n) - 0.5).astype(np.complex128)
+    v1 /= np.sqrt(np.vdot(v1, v1).real)
+    alpha = np.zeros(max_niter)
+    beta = np.zeros(max_niter + 1)                     # beta[0] is beta(0) = 0
+    evals = np.zeros(nev)
+    kvec = None
+    nkrylov = 0
+    curr, prev = v1.copy(), np.zeros(n, dtype=np.complex128)
+    for i in range(1, max_niter + 1):
+        prev = -beta[i - 1] * prev
+        prev = matvec(csr, curr, prev)
+        alpha[i - 1] = np.vdot(curr, prev).real
+        if i % 10 == 0 or i == max_niter:
+            ke, kv = _tridiag_eigs(alpha[:i], beta[1:i])
+            ke = np.concatenate([ke, np.zeros(max(0, nev - i))])
+            if i >= nev:
+                if abs(ke[nev - 1] - evals[nev - 1]) < eval_tol:
+                    evals = ke[:nev].copy()
+                    nkrylov, kvec = i, kv
+                    break
+            evals = ke[:nev].copy()
+        prev = prev - alpha[i - 1] * curr
+        beta[i] = np.sqrt(np.vdot(prev, prev).real)
+        if abs(beta[i]) < 1e-10:
+            if i >= 2:
+                ke, kvec = _tridiag_eigs(alpha[:i], beta[1:i])
+                ke = np.concatenate([ke, np.zeros(max(0, nev - i))])
+                evals = ke[:nev].copy()
+            else:
+                evals[0] = alpha[0]
+                kvec = np.ones((1, 1))
+            nkrylov = i
+            break
+        prev = prev / beta[i]
+        curr, prev = prev, curr
+    evec = np.zeros((n, nvec), dtype=np.complex128)
+    curr, prev = v1.copy(), np.zeros(n, dtype=np.complex128)
+    for i in range(1, nkrylov + 1):
+        m = min(nvec, kvec.shape[1])
+        evec[:, :m] += np.outer(curr, kvec[i - 1, :m])
+        if i < nkrylov:
+            prev = -alpha[i - 1] * curr - beta[i - 1] * prev
+            prev = matvec(csr, curr, prev)
+            prev = prev / beta[i]
+            curr, prev = prev, curr
+    return evals, evec, nkrylov

@@ -111,6 +111,64 @@ def test_known_answer_eigenvalues(golden_dir):
     assert np.abs(e - expected).max() < 1e-10
 
 
+def _known_answer_hamiltonian(golden_dir):
+    d = os.path.join(golden_dir, "known_answer")
+    fock = orc.read_fock(os.path.join(d, "fock_i.in"))
+    csr = orc.build_csr("ham_i", fock, orc.read_terms(os.path.join(d, "hopping_i.in"), 2),
+                        orc.read_terms(os.path.join(d, "coulomb_i.in"), 4), num_val_orbs=20)
+    return csr, np.loadtxt(os.path.join(d, "expected_eigvals.txt"))
+
+
+def test_plain_lanczos_known_answer(golden_dir):
+    """ed_solver = 1 (lanczos.f90:6-167) on the 45 states of test_fortran.py:8-42.
+
+    Without reorthogonalisation a Krylov space holds one vector per distinct level, so the
+    recurrence breaks down (beta < 1e-10) after as many steps as there are distinct levels
+    (11), and the lowest nev eigenvalues it reports are the lowest DISTINCT levels: the
+    9-fold ground level appears once. ZHEEV (ed_solver = 0) and ARPACK (ed_solver = 2) report
+    it nine times."""
+    csr, expected = _known_answer_hamiltonian(golden_dir)
+    levels = expected[np.r_[True, np.diff(expected) > 1e-8]]
+    H = csr.dense()
+    e, v, nkrylov = orc.lanczos_eigs(csr, 3, 500, 1e-8, nvec=3, seed=1)
+    assert nkrylov == levels.size
+    assert np.abs(e - levels[:3]).max() < 1e-10
+    for j in range(3):
+        assert abs(np.linalg.norm(v[:, j]) - 1.0) < 1e-10
+        assert np.linalg.norm(H @ v[:, j] - e[j] * v[:, j]) < 1e-10
+
+
+def test_plain_lanczos_converges_on_check_steps(dense_small):
+    """Convergence is tested every 10 steps on the change of the nev-th eigenvalue
+    (lanczos.f90:89-110); eigenvectors come from re-running the recurrence (:133-157)."""
+    g = dense_small
+    csr = orc.build_csr("ham_i", g["fock_i"], (g["hop_i_idx"], g["hop_i_val"]), (g["coul_i_idx"], g["coul_i_val"]),
+                        num_val_orbs=int(g["nv"]))
+    H = csr.dense()
+    exact = np.linalg.eigvalsh(H)
+    for seed in (0, 1):
+        e, v, nkrylov = orc.lanczos_eigs(csr, 3, 500, 1e-8, nvec=2, seed=seed)
+        assert nkrylov % 10 == 0 and nkrylov < csr.nrows
+        assert np.abs(e - exact[:3]).max() < 1e-9
+        for j in range(2):
+            assert np.linalg.norm(H @ v[:, j] - e[j] * v[:, j]) < 1e-8
+        # the start vector is real: so are the Lanczos vectors of this real symmetric H
+        if np.abs(H.imag).max() == 0:
+            assert np.abs(v.imag).max() == 0
+
+
+def test_plain_lanczos_without_convergence_gives_zero_vectors(dense_small):
+    """When max_niter passes before the test succeeds, nkrylov stays 0 in the reference and the
+    eigenvector pass (lanczos.f90:133-157) runs no step: the vectors are zero, the eigenvalues
+    those of the last check."""
+    g = dense_small
+    csr = orc.build_csr("ham_i", g["fock_i"], (g["hop_i_idx"], g["hop_i_val"]), (g["coul_i_idx"], g["coul_i_val"]),
+                        num_val_orbs=int(g["nv"]))
+    e, v, nkrylov = orc.lanczos_eigs(csr, 1, 9, 1e-14, nvec=1)
+    assert nkrylov == 0 and not v.any()
+    assert e[0] > np.linalg.eigvalsh(csr.dense())[0]
+
+
 def test_spectra_and_boltzmann(golden_dir):
     with np.load(os.path.join(golden_dir, "spectra.npz")) as z:
         g = {k: z[k] for k in z.files}

@@ -157,6 +157,60 @@ def test_abi_error_path_without_gpu():
         _lib.call("edx_fock_count", -1, 0, ctypes.byref(n))
 
 
+def _no_cuda_device():
+    try:
+        import torch
+        return not torch.cuda.is_available()
+    except ImportError:
+        return True
+
+
+@pytest.mark.skipif(not _no_cuda_device(), reason="host-validation test; runs where no GPU is visible")
+def test_every_entry_point_rejects_null_arguments():
+    """The reference STOPs on bad input (src/io.f90:37-39); every libedx entry point instead
+    returns EDX_ERR_INVALID with a message, here for an argument list of NULLs and zeros."""
+    import ctypes
+    from edrixs_b200 import _lib
+    _lib.load()
+    raw = ctypes.CDLL(_lib.LIB_PATH)          # no argtypes: zeros in every slot
+    raw.edx_last_error.restype = ctypes.c_char_p
+    txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "edx.h")).read(), flags=re.S)
+    entries = re.findall(r"^int (edx_\w+)\s*\((.*?)\);", txt, flags=re.M | re.S)
+    checked = 0
+    for name, params in entries:
+        nargs = len([p for p in params.split(",") if p.strip() and p.strip() != "void"])
+        if nargs == 0:
+            continue
+        rc = getattr(raw, name)(*([None] * nargs))
+        assert rc == 1, (name, rc)
+        assert raw.edx_last_error(), name
+        checked += 1
+    assert checked >= 30
+
+
+@pytest.mark.skipif(not _no_cuda_device(), reason="host-validation test; runs where no GPU is visible")
+def test_matrix_descriptors_are_validated_on_the_host():
+    import ctypes
+    from edrixs_b200 import _lib
+    L = _lib.load()
+    nbytes = ctypes.c_size_t(0)
+    A = _lib.Csr(nrows=-5, ncols=10, nnz=0)
+    assert L.edx_spmm(ctypes.byref(A), 1, 0, None, 1, None, 1, 1.0, 0, 0, 0, 0, 0, 0, None) == 1
+    assert b"negative" in L.edx_last_error()
+    A = _lib.Csr(nrows=5, ncols=5, nnz=3)
+    assert L.edx_spmm(ctypes.byref(A), 1, 0, None, 1, None, 1, 1.0, 0, 0, 0, 0, 0, 0, None) == 1
+    assert b"row pointers" in L.edx_last_error()
+    assert L.edx_pack_workspace(ctypes.byref(A), ctypes.byref(nbytes)) == 1
+    assert L.edx_krylov_workspace(100, 0, None, 10, ctypes.byref(nbytes)) == 1
+    assert L.edx_krylov_workspace(-1, 4, None, 10, ctypes.byref(nbytes)) == 1
+    assert L.edx_krylov_workspace(100, 4, None, 10, ctypes.byref(nbytes)) == 0 and nbytes.value > 0
+    n = ctypes.c_int64(0)
+    assert L.edx_fock_count(63, 31, ctypes.byref(n)) == 0 and n.value == 916312070471295267  # C(63,31)
+    assert L.edx_fock_count(0, 0, ctypes.byref(n)) == 0 and n.value == 1
+    assert L.edx_fock_count(64, 32, ctypes.byref(n)) == 1
+    assert L.edx_fock_count(10, 11, ctypes.byref(n)) == 1
+
+
 # ---- workload generator ------------------------------------------------------------------
 
 def test_siam_seeded_and_hermitian():

@@ -25,6 +25,9 @@ What it writes (all small):
                      pure-Python Kramers-Heisenberg solvers (xas_1v1c_py, rixs_1v1c_py on
                      ed_1v1c_py eigenstates) and the input files its Fortran-path callers write
                      for the same ion; also a thermal case (3 ground states at 3000 K).
+  search_gs/         the reference's ground-state search over N (ed_siam_fort, do_ed=0) for a
+                     p shell with one bath site: its term files, the N of every solver call,
+                     search_gs.log and search_result.dat (solver calls answered by the oracle).
 """
 import hashlib
 import json
@@ -388,6 +391,62 @@ def denmat_golden(ed, dense_path, out_path):
     return float(e[1] - e[0]), float(e[2] - e[1])
 
 
+def search_gs(ed, out_dir, level=-6.0):
+    """The reference's ground-state search over N (ed_siam_fort with do_ed=0,
+    edrixs/solvers.py:2156-2263) on a p shell with one bath site (6 + 6 orbitals, N = 0..12,
+    at most 924 states), general hybridisation (siam_type=1). Its
+    ed_fsolver calls go to a stand-in that solves with the oracle (dense) and writes
+    eigvals.dat / denmat.dat in the reference's formats; the reference's own loop reads them
+    back, walks N, and writes search_gs.log and search_result.dat.  Kept: hopping_i.in and
+    coulomb_i.in of the first call, the N of every call, both result files, and config.in of
+    the last call (the one at the ground-state occupancy)."""
+    from edrixs_b200 import io as edxio
+    from oracle import pyoracle as orc
+    rng = np.random.default_rng(5)
+    a = rng.normal(0.0, 0.3, (6, 6)) + 1j * rng.normal(0.0, 0.3, (6, 6))
+    hopping = np.zeros((12, 12), dtype=np.complex128)
+    hopping[:6, :6] = (a + a.conj().T) / 2 + level * np.eye(6)
+    hopping[6:, 6:] = np.diag(rng.uniform(-2.0, 2.0, 6))
+    hopping[:6, 6:] = rng.normal(0.0, 0.6, (6, 6)) + 1j * rng.normal(0.0, 0.6, (6, 6))
+    hopping[6:, :6] = hopping[:6, 6:].conj().T
+    calls = []
+
+    def ed_fsolver(comm, my_id, num_procs):
+        cfg = edxio.read_config("config.in")
+        fock = orc.read_fock("fock_i.in")
+        if not calls:
+            os.makedirs(out_dir, exist_ok=True)
+            for fn in ("hopping_i.in", "coulomb_i.in"):
+                shutil.copy(fn, os.path.join(out_dir, fn))
+        calls.append(bin(int(fock[0])).count("1"))
+        nv = cfg["num_val_orbs"]
+        H = orc.build_csr("ham_i", fock, orc.read_terms("hopping_i.in", 2), orc.read_terms("coulomb_i.in", 4),
+                          num_val_orbs=nv)
+        e, v = np.linalg.eigh(H.dense())
+        nvec = min(cfg["nvector"], len(fock))
+        edxio.write_eigvals("eigvals.dat", e[:min(cfg["neval"], len(fock))])
+        edxio.write_denmat("denmat.dat", np.stack([orc.denmat(fock, nv, v[:, k]) for k in range(nvec)]))
+        shutil.copy("config.in", os.path.join(out_dir, "config_last.in"))
+
+    mod = types.ModuleType("edrixs.fedrixs")
+    mod.ed_fsolver = ed_fsolver
+    sys.modules["edrixs.fedrixs"] = mod
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as td:
+        os.chdir(td)
+        try:
+            eval_i, denmat, noccu = ed.ed_siam_fort(FakeComm(), ("p", "s"), 1, siam_type=1, hopping=hopping,
+                                                   slater=([4.0, 3.0], [4.0, 3.0]), do_ed=0,
+                                                   ed_solver=2, neval=2, nvector=1, min_ndim=10)
+            for fn in ("search_gs.log", "search_result.dat"):
+                shutil.copy(fn, os.path.join(out_dir, fn))
+        finally:
+            os.chdir(cwd)
+    with open(os.path.join(out_dir, "calls.json"), "w") as f:
+        json.dump({"n_per_call": calls, "noccu_gs": int(noccu), "eval_i": [float(x) for x in eval_i]}, f)
+    return calls, int(noccu)
+
+
 def main(ref):
     ed = import_reference(ref)
     known_answer(ed, os.path.join(HERE, "known_answer"))
@@ -397,6 +456,7 @@ def main(ref):
     siam_callers(ed, os.path.join(HERE, "siam_callers"))
     print("kh_1v1c", kh_1v1c(ed, os.path.join(HERE, "kh_1v1c")))
     print("denmat", denmat_golden(ed, os.path.join(HERE, "dense_small.npz"), os.path.join(HERE, "denmat.npz")))
+    print("search_gs", search_gs(ed, os.path.join(HERE, "search_gs")))
     print("golden fixtures written to", HERE)
 
 

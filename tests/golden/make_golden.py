@@ -25,6 +25,9 @@ What it writes (all small):
                      pure-Python Kramers-Heisenberg solvers (xas_1v1c_py, rixs_1v1c_py on
                      ed_1v1c_py eigenstates) and the input files its Fortran-path callers write
                      for the same ion; also a thermal case (3 ground states at 3000 K).
+  callers_2v1c/      the files ed_2v1c_fort, xas_2v1c_fort (dipole and quadrupole) and
+                     rixs_2v1c_fort write for t2g + p valence shells and an s core, and the dense
+                     matrices two_fermion / four_fermion build from the same terms.
   search_gs/         the reference's ground-state search over N (ed_siam_fort, do_ed=0) for a
                      p shell with one bath site: its term files, the N of every solver call,
                      search_gs.log and search_result.dat (solver calls answered by the oracle).
@@ -391,6 +394,123 @@ def denmat_golden(ed, dense_path, out_path):
     return float(e[1] - e[0]), float(e[2] - e[1])
 
 
+def callers_2v1c(ed, out_dir):
+    """Two valence shells and one core shell: t2g (6) + p (6) valence orbitals, an s core (2),
+    10 valence electrons (66 initial, 2 x 12 intermediate states).  The files that
+    ed_2v1c_fort (do_ed=False), xas_2v1c_fort (a p<-s dipole and a t2g<-s quadrupole
+    operator) and rixs_2v1c_fort write, captured with a recording stand-in for
+    edrixs.fedrixs, and the dense matrices the reference's manybody_operator.two_fermion /
+    four_fermion build from the same terms (H_i, H_n, each transition operator), on bases
+    ordered like the Fortran rows (core-major intermediate index, src/ham.f90:424-446)."""
+    rng = np.random.default_rng(23)
+    a = rng.normal(scale=0.2, size=(6, 6)) + 1j * rng.normal(scale=0.2, size=(6, 6))
+    hv = rng.normal(scale=0.3, size=(6, 6)) + 1j * rng.normal(scale=0.3, size=(6, 6))
+    shells = ("t2g", "p", "s")
+    kw = dict(shell_level=(0.0, 2.0, -40.0), v1_soc=(0.05, 0.06), v2_soc=(0.02, 0.03), v_tot_noccu=10,
+              slater=([4.0, 3.0, 2.0, 2.0, 1.0, 0.8, 0.5, 1.5, 1.0],
+                      [4.0, 3.0, 2.0, 2.0, 1.0, 0.8, 0.5, 1.5, 1.0, 2.0, 0.7, 1.8, 0.6]),
+              v1_cfmat=a + a.conj().T, hopping_v1v2=hv)
+    calls = {"n": 0}
+
+    def recorder(kind):
+        def fsolver(comm, my_id, num_procs):
+            calls["n"] += 1
+            d = os.path.join(out_dir, f"{kind}_{calls['n']:02d}")
+            os.makedirs(d, exist_ok=True)
+            for fn in os.listdir("."):
+                if fn.endswith(".in"):
+                    shutil.copy(fn, os.path.join(d, fn))
+            with open(f"{kind}_poles.1", "w") as f:
+                f.write("#number_of_poles:            1\n#enegry:                  0.0\n"
+                        "#normalization:           1.0\n    1      0.0      0.0\n")
+        return fsolver
+
+    mod = types.ModuleType("edrixs.fedrixs")
+    mod.ed_fsolver, mod.xas_fsolver, mod.rixs_fsolver = recorder("ed"), recorder("xas"), recorder("rixs")
+    sys.modules["edrixs.fedrixs"] = mod
+    if os.path.isdir(out_dir):
+        shutil.rmtree(out_dir)
+    os.makedirs(out_dir)
+    cwd = os.getcwd()
+    geo = dict(thin=0.5, phi=0.2)
+    with tempfile.TemporaryDirectory() as td:
+        os.chdir(td)
+        try:
+            comm = FakeComm()
+            ed.ed_2v1c_fort(comm, shells, do_ed=False, ed_solver=0, neval=2, nvector=1, min_ndim=1000, **kw)
+            d = os.path.join(out_dir, "ed_00")
+            os.makedirs(d)
+            for fn in os.listdir("."):
+                if fn.endswith(".in"):
+                    shutil.copy(fn, os.path.join(d, fn))
+            om = np.linspace(-2.0, 8.0, 5)
+            ed.xas_2v1c_fort(comm, shells, om, gamma_c=0.3, v_tot_noccu=10, trans_to_which=2,
+                             pol_type=[("linear", 0.0)], num_gs=1, nkryl=100, **geo)
+            ed.xas_2v1c_fort(comm, shells, om, gamma_c=0.3, v_tot_noccu=10, trans_to_which=1,
+                             pol_type=[("linear", 0.3)], num_gs=1, nkryl=100, **geo)
+            ed.rixs_2v1c_fort(comm, shells, np.array([1.0, 3.0]), np.linspace(-0.5, 4.0, 5), gamma_c=0.5,
+                              gamma_f=0.1, v_tot_noccu=10, trans_to_which=2, thout=1.0,
+                              pol_type=[("linear", 0.0, "linear", np.pi / 2)], num_gs=1, nkryl=100,
+                              linsys_max=500, linsys_tol=1e-12, **geo)
+        finally:
+            os.chdir(cwd)
+    base = os.path.join(out_dir, "ed_00")
+    for d in sorted(os.listdir(out_dir)):
+        if d == "ed_00":
+            continue
+        for fn in os.listdir(os.path.join(out_dir, d)):
+            p = os.path.join(out_dir, d, fn)
+            q = os.path.join(base, fn)
+            stale = d.startswith("rixs") and fn == "transop_xas.in"   # left by the XAS calls
+            if stale or (os.path.exists(q) and open(p, "rb").read() == open(q, "rb").read()):
+                os.remove(p)
+
+    # dense matrices from the reference's operator builders on the recorded terms
+    def terms(path, nidx):
+        with open(path) as f:
+            n = int(f.readline().split()[0])
+            rows = [f.readline().split() for _ in range(n)]
+        return ([[int(r[k]) for k in range(nidx)] for r in rows],
+                [float(r[nidx]) + 1j * float(r[nidx + 1]) for r in rows])
+
+    def tensor(tm, n, nidx):
+        t = np.zeros((n,) * nidx, dtype=complex)
+        for idx, v in zip(*tm):
+            t[tuple(i - 1 for i in idx)] += v
+        return t
+
+    nv, nc, N = 12, 2, 10
+    ntot = nv + nc
+    fock_i = np.array(sorted(ed.get_fock_full_N(nv, N)), dtype=np.int64)
+    fock_n = np.array(sorted(ed.get_fock_full_N(nv, N + 1)), dtype=np.int64)
+    core_full = (1 << nc) - 1
+    fock_core = [core_full - (1 << (nc - 1 - k)) for k in range(nc)]
+    basis_i = [bits(s, nv) for s in fock_i]
+    basis_i_fullcore = [bits((core_full << nv) | s, ntot) for s in fock_i]
+    basis_n = [bits((fc << nv) | s, ntot) for fc in fock_core for s in fock_n]
+    ed0 = os.path.join(out_dir, "ed_00")
+    H_i = (ed.two_fermion(tensor(terms(os.path.join(ed0, "hopping_i.in"), 2), ntot, 2)[:nv, :nv], basis_i) +
+           ed.four_fermion(tensor(terms(os.path.join(ed0, "coulomb_i.in"), 4), ntot, 4)[:nv, :nv, :nv, :nv],
+                           basis_i))
+    H_n = (ed.two_fermion(tensor(terms(os.path.join(ed0, "hopping_n.in"), 2), ntot, 2), basis_n) +
+           ed.four_fermion(tensor(terms(os.path.join(ed0, "coulomb_n.in"), 4), ntot, 4), basis_n))
+    mats = {"H_i": H_i, "H_n": H_n}
+    for d in sorted(os.listdir(out_dir)):
+        for fn, rows, cols, name in (("transop_xas.in", basis_n, basis_i_fullcore, "D"),
+                                     ("transop_rixs_i.in", basis_n, basis_i_fullcore, "D_in"),
+                                     ("transop_rixs_f.in", basis_i_fullcore, basis_n, "D_out")):
+            p = os.path.join(out_dir, d, fn)
+            if os.path.exists(p):
+                mats[f"{name}_{d}"] = ed.two_fermion(tensor(terms(p, 2), ntot, 2), rows, cols)
+    data = {}
+    for name, M in mats.items():
+        r, c = np.nonzero(M)
+        data[f"{name}_row"], data[f"{name}_col"] = r.astype(np.int32), c.astype(np.int32)
+        data[f"{name}_val"], data[f"{name}_shape"] = M[r, c], np.array(M.shape)
+    np.savez_compressed(os.path.join(out_dir, "dense.npz"), **data)
+    return sorted(os.listdir(out_dir)), sorted(mats)
+
+
 def search_gs(ed, out_dir, level=-6.0):
     """The reference's ground-state search over N (ed_siam_fort with do_ed=0,
     edrixs/solvers.py:2156-2263) on a p shell with one bath site (6 + 6 orbitals, N = 0..12,
@@ -456,6 +576,7 @@ def main(ref):
     siam_callers(ed, os.path.join(HERE, "siam_callers"))
     print("kh_1v1c", kh_1v1c(ed, os.path.join(HERE, "kh_1v1c")))
     print("denmat", denmat_golden(ed, os.path.join(HERE, "dense_small.npz"), os.path.join(HERE, "denmat.npz")))
+    print("callers_2v1c", callers_2v1c(ed, os.path.join(HERE, "callers_2v1c")))
     print("search_gs", search_gs(ed, os.path.join(HERE, "search_gs")))
     print("golden fixtures written to", HERE)
 

@@ -44,8 +44,9 @@ def _path(name):
     return os.path.join(os.getcwd(), name)
 
 
-def _ed_core(cfg, H, basis):
-    """Solve per src/ed_driver.f90:65-181 and return (eigvals, eigvecs (n, nvector))."""
+def ed_core(cfg, H):
+    """Lowest eigenpairs of H as src/ed_driver.f90:65-181 chooses them from config.in's
+    ed_solver / min_ndim / neval / nvector / eigval_tol: (eigvals, eigvecs (n, nvector))."""
     ndim = H.nrows
     ed_solver = cfg["ed_solver"]
     if ndim < cfg["min_ndim"]:
@@ -72,7 +73,7 @@ def ed_fsolver(comm=0, my_id=0, num_procs=1):
     fock = edxio.read_fock(_path("fock_i.in"))
     basis = device.basis_from_states(fock)
     H = device.build_csr(device.HAM_I, basis, hop, coul, num_val_orbs=cfg["num_val_orbs"])
-    e, v = _ed_core(cfg, H, basis)
+    e, v = ed_core(cfg, H)
     edxio.write_eigvals(_path("eigvals.dat"), e)
     nv = cfg["num_val_orbs"]
     dm = device.denmat(basis, nv, v).cpu().numpy()

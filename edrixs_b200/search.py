@@ -60,7 +60,7 @@ def device_solver(hopping, coulomb, ntot_v, v_norb, *, maxiter=1000, eigval_tol=
     lowest eigenpair (the ED core of ed_fsolver with ed_solver=1, neval=nvector=1) and the
     density matrix of that eigenvector."""
     from . import device
-    from .fedrixs import _ed_core
+    from .fedrixs import ed_core
     device.require_cuda()
     cfg = {"ed_solver": 1, "neval": 1, "nvector": 1, "maxiter": maxiter, "eigval_tol": eigval_tol,
            "min_ndim": min_ndim}
@@ -68,7 +68,7 @@ def device_solver(hopping, coulomb, ntot_v, v_norb, *, maxiter=1000, eigval_tol=
     def solve(N):
         basis = device.fock_unrank(ntot_v, N)
         H = device.build_csr(device.HAM_I, basis, hopping, coulomb, num_val_orbs=ntot_v)
-        e, v = _ed_core(cfg, H, basis)
+        e, v = ed_core(cfg, H)
         dm = device.denmat(basis, ntot_v, v).cpu().numpy()
         return file_rounded(e[0]), impurity_occupancy(dm[0], v_norb)
 

@@ -246,3 +246,28 @@ def test_admission_estimates_and_oversize_rejection():
     assert isinstance(f, Future) and isinstance(f.exception(timeout=1), MemoryError)
     f2 = srv.submit(small)
     assert not f2.done() and len(srv.waiting) == 1
+
+
+def test_product_package_never_imports_the_oracle():
+    """The oracle is test infrastructure: no module of the product package imports it, so no
+    product call can route through it (bench.py's CPU-baseline leg and smoke()'s checker are
+    the only other importers)."""
+    import ast
+    pkg = os.path.join(ROOT, "edrixs_b200")
+    offenders = []
+    for dirpath, dirnames, filenames in os.walk(pkg):
+        dirnames[:] = [d for d in dirnames if not d.startswith("_build")]
+        for fn in filenames:
+            if not fn.endswith(".py"):
+                continue
+            path = os.path.join(dirpath, fn)
+            tree = ast.parse(open(path).read(), filename=path)
+            for node in ast.walk(tree):
+                names = []
+                if isinstance(node, ast.Import):
+                    names = [a.name for a in node.names]
+                elif isinstance(node, ast.ImportFrom) and node.module:
+                    names = [node.module]
+                if any(n == "oracle" or n.startswith("oracle.") for n in names):
+                    offenders.append(os.path.relpath(path, ROOT))
+    assert not offenders, offenders

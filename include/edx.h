@@ -186,10 +186,11 @@ int edx_tiles_fill(const edx_csr* A, edx_tiles* T, void* d_work, size_t work_byt
 /* ---------------------------------------------------------------------------------- */
 
 /* A Hamiltonian built from a few hundred hopping and Coulomb terms has only a few hundred
- * distinct off-diagonal values (for example 418 in the 11.2 M entries of a 184,756-state
- * impurity model).  The packed form keeps the diagonal as a dense complex128 vector and
- * stores every off-diagonal entry by its column and an index into vals (the distinct values,
- * bit-exact copies).  Rows keep the CSR's column order.  Two forms:
+ * distinct off-diagonal values (for example 423 bit patterns in the 11.0 M off-diagonal
+ * entries of a 184,756-state impurity model).  The packed form keeps the diagonal as a
+ * dense complex128 vector and stores every off-diagonal entry by its column and an index
+ * into vals (the distinct values, bit-exact copies).  Rows keep the CSR's column order.
+ * Two forms:
  *   narrow (vbits >= 1): one 32-bit word, ent = column << vbits | index, with
  *     vbits = 32 - (bits of ncols-1); it exists when nval <= min(2^vbits, EDX_PACK_VALUES_MAX);
  *   wide (vbits == 0): ent = column and vidx = index (16 bits), 6 bytes per entry, for
@@ -327,9 +328,10 @@ typedef struct edx_krylov_opts {
 
 /* k independent Lanczos recurrences of build_krylov_mp (src/lanczos.f90:210-303), run
  * together so that every iteration is one SpMM over k columns (FP64 recurrence).  d_v0:
- * n x k start vectors, row-major with leading dimension opts->v0_ld (k when 0).  Outputs for column j: d_alpha[j*maxn + i],
- * d_beta[j*maxn + i] (i < neff), d_norm[j] = <v0_j|v0_j>, d_neff[j].  Column j stops when
- * beta < 1e-10 (absolute, :291).  The matrix may be complex128 or complex64 (vectors and
+ * n x k start vectors, row-major with leading dimension opts->v0_ld (k when 0).  Outputs
+ * for column j: d_alpha[j*maxn + i], d_beta[j*maxn + i] (i < neff), d_norm[j] =
+ * <v0_j|v0_j>, d_neff[j].  Column j stops when beta < 1e-10 (absolute, :291); a zero start
+ * vector gives neff = 1 and norm 0.  The matrix may be complex128 or complex64 (vectors and
  * scalars stay complex128 / FP64). */
 int edx_krylov_workspace(int64_t n, int k, const edx_krylov_opts* opts, int maxn, size_t* bytes);
 int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn, double* d_alpha,

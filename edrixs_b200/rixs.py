@@ -15,7 +15,10 @@ Here:
     (libedx edx_krylov shifts) and stopped by the reference's own rule;
  3. every Lanczos vector is pushed through each D_out^+(pol_out) while it is hot in L2
     (edx_krylov projections), so x_z never has to exist: D_out^+ x_z = (D_out^+ V) y_z is
-    a batched ZGEMM;
+    a batched ZGEMM.  When the projected vectors would not fit in memory (``stream``), a
+    second Krylov pass regenerates the same Lanczos vectors (deterministic reductions) and
+    folds each D_out^+ v_i into the final-state start vectors, a window of
+    ``stream_window`` steps at a time (edx_krylov proj_window);
  4. all #pol_out x #pol_in x #gs x #omega final-state Lanczos runs on H_f go as one block
     of columns (one SpMM per step);
  5. continued fractions for every pole set on the energy-loss grid (edx_cf_spectrum) and

@@ -13,6 +13,9 @@
 * Continuous batching: several worker threads, each with its own CUDA stream, run admitted
   work concurrently; a request that arrives while others run is admitted as soon as memory
   and a worker free up.  Every request records its queueing and service latency.
+* Cancellation: a caller may cancel a request's Future while the request waits; it then
+  leaves the queue (and any coalesced solve).  Once its solve starts it can no longer be
+  cancelled (concurrent.futures semantics).
 """
 import itertools
 import math
@@ -255,6 +258,8 @@ class Server:
             with self.cv:
                 if self.stop_flag:
                     return
+                # requests whose callers cancelled them (Future.cancel) leave the queue
+                self.waiting = [(r, f) for r, f in self.waiting if not f.cancelled()]
                 if self.free_workers == 0 or not self.waiting:
                     self.cv.wait(timeout=0.05)
                     continue
@@ -278,6 +283,12 @@ class Server:
                     for r2, f2 in self.waiting:
                         (group if coalesce_key(r2) == sig else rest).append((r2, f2))
                     self.waiting = rest
+                # a future marked running can no longer be cancelled; one cancelled since the
+                # purge above is dropped here
+                group = [(r, f) for r, f in group if f.set_running_or_notify_cancel()]
+                if not group:
+                    continue
+                req = group[0][0]
                 need = sum(estimate_bytes(r, r.model in self.residents) for r, _ in group)
                 res = self._resident(req.model)
                 res.busy += 1

@@ -94,3 +94,57 @@ def test_scheduler_groups_waiting_requests_when_a_worker_frees():
     srv.jobs.put(None)
     assert groups[1] == [a.id, b.id]  # same Hamiltonian and settings: one solve
     assert sorted(map(tuple, groups[2:])) == sorted([(x.id,), (c.id,)])
+
+
+def test_cancelled_requests_leave_the_queue_and_the_coalesced_solve():
+    """Future.cancel() on a waiting request removes it: it is not dispatched, and the requests
+    it would have been coalesced with still run.  A dispatched request can no longer be
+    cancelled.  (No GPU: a fake worker takes the jobs.)"""
+    import threading
+    import time
+    from edrixs_b200.serve import ModelSpec, Request, Server
+    srv = Server(hbm_budget=1e12, workers=1)
+    groups = []
+    release = threading.Event()
+
+    def fake_worker():
+        while True:
+            job = srv.jobs.get()
+            if job is None:
+                return
+            group, res, need = job
+            groups.append([r.id for r, _ in group])
+            release.wait(5)
+            with srv.cv:
+                res.busy -= 1
+                srv.inflight_bytes -= need
+                srv.free_workers += 1
+                srv.cv.notify_all()
+
+    sched = threading.Thread(target=srv._schedule, daemon=True)
+    worker = threading.Thread(target=fake_worker, daemon=True)
+    sched.start()
+    worker.start()
+    m, m2 = ModelSpec(4, 7, 1), ModelSpec(4, 7, 2)
+    el = np.linspace(-0.5, 12.0, 100)
+    first = Request("ed", m2)
+    f_first = srv.submit(first)
+    time.sleep(0.3)
+    assert groups == [[first.id]] and not f_first.cancel()   # running: not cancellable
+    a = Request("rixs", m, ngs=1, omegas=np.array([1.0]), eloss=el, pols=(0,))
+    b = Request("rixs", m, ngs=2, omegas=np.array([2.0]), eloss=el, pols=(1,))
+    c = Request("ed", m)
+    fa, fb, fc = srv.submit(a), srv.submit(b), srv.submit(c)
+    assert fa.cancel() and fc.cancel()
+    release.set()
+    deadline = time.time() + 5
+    while len(groups) < 2 and time.time() < deadline:
+        time.sleep(0.05)
+    time.sleep(0.3)
+    with srv.cv:
+        srv.stop_flag = True
+        srv.cv.notify_all()
+    srv.jobs.put(None)
+    assert groups == [[first.id], [b.id]]
+    assert fa.cancelled() and fc.cancelled() and fb.running()
+    assert srv.waiting == [] and srv.free_workers == 1 and srv.inflight_bytes == 0

@@ -21,7 +21,7 @@ import torch
 
 from . import device
 from . import io as edxio
-from . import solvers
+from . import solvers, trace
 
 
 class FakeComm:
@@ -72,11 +72,14 @@ def ed_fsolver(comm=0, my_id=0, num_procs=1):
     coul = edxio.read_coulomb(_path("coulomb_i.in"))
     fock = edxio.read_fock(_path("fock_i.in"))
     basis = device.basis_from_states(fock)
-    H = device.build_csr(device.HAM_I, basis, hop, coul, num_val_orbs=cfg["num_val_orbs"])
-    e, v = ed_core(cfg, H)
+    with trace.phase("ed: build H_i"):
+        H = device.build_csr(device.HAM_I, basis, hop, coul, num_val_orbs=cfg["num_val_orbs"])
+    with trace.phase("ed: eigenpairs"):
+        e, v = ed_core(cfg, H)
     edxio.write_eigvals(_path("eigvals.dat"), e)
     nv = cfg["num_val_orbs"]
-    dm = device.denmat(basis, nv, v).cpu().numpy()
+    with trace.phase("ed: density matrix"):
+        dm = device.denmat(basis, nv, v).cpu().numpy()
     edxio.write_denmat(_path("denmat.dat"), dm)
     if cfg["idump"]:
         vh = v.cpu().numpy()
@@ -109,10 +112,13 @@ def xas_fsolver(comm=0, my_id=0, num_procs=1):
     nv, nc = cfg["num_val_orbs"], cfg["num_core_orbs"]
     num_gs = cfg["num_gs"]
     evals, g = _read_gs(num_gs, fi.ndim)
-    D = device.build_csr(device.TRANS_I, fn, trans, right=fi, num_val_orbs=nv, num_core_orbs=nc)
-    phi = device.spmm(D, torch.from_numpy(g).cuda())
-    Hn = device.build_csr(device.HAM_N, fn, hop_n, coul_n, num_val_orbs=nv, num_core_orbs=nc)
-    r = device.krylov(Hn, phi, cfg["nkryl"])
+    with trace.phase("xas: D|g>"):
+        D = device.build_csr(device.TRANS_I, fn, trans, right=fi, num_val_orbs=nv, num_core_orbs=nc)
+        phi = device.spmm(D, torch.from_numpy(g).cuda())
+    with trace.phase("xas: build H_n"):
+        Hn = device.build_csr(device.HAM_N, fn, hop_n, coul_n, num_val_orbs=nv, num_core_orbs=nc)
+    with trace.phase("xas: Krylov"):
+        r = device.krylov(Hn, phi, cfg["nkryl"])
     _write_poles("xas_poles", r, evals)
 
 
@@ -147,20 +153,26 @@ def rixs_fsolver(comm=0, my_id=0, num_procs=1):
     nv, nc = cfg["num_val_orbs"], cfg["num_core_orbs"]
     num_gs = cfg["num_gs"]
     evals, g = _read_gs(num_gs, fi.ndim)
-    Din = device.build_csr(device.TRANS_I, fn, tr_i, right=fi, num_val_orbs=nv, num_core_orbs=nc)
-    phi = device.spmm(Din, torch.from_numpy(g).cuda())
-    Hn = device.build_csr(device.HAM_N, fn, hop_n, coul_n, num_val_orbs=nv, num_core_orbs=nc)
+    with trace.phase("rixs: D_in|g>"):
+        Din = device.build_csr(device.TRANS_I, fn, tr_i, right=fi, num_val_orbs=nv, num_core_orbs=nc)
+        phi = device.spmm(Din, torch.from_numpy(g).cuda())
+    with trace.phase("rixs: build H_n"):
+        Hn = device.build_csr(device.HAM_N, fn, hop_n, coul_n, num_val_orbs=nv, num_core_orbs=nc)
     xs = []
-    for igs in range(num_gs):
-        z = complex(cfg["omega_in"] + evals[igs], cfg["gamma_in"])
-        x, it, res = device.minres(Hn, phi[:, igs].contiguous(), cfg["linsys_tol"], cfg["linsys_max"], alpha=-1.0,
-                                   sigma=z)
-        xs.append(x)
+    with trace.phase("rixs: MINRES"):
+        for igs in range(num_gs):
+            z = complex(cfg["omega_in"] + evals[igs], cfg["gamma_in"])
+            x, it, res = device.minres(Hn, phi[:, igs].contiguous(), cfg["linsys_tol"], cfg["linsys_max"],
+                                       alpha=-1.0, sigma=z)
+            xs.append(x)
     X = torch.stack(xs, dim=1)
-    Dout = device.build_csr(device.TRANS_F, ff, tr_f, right=fn, num_val_orbs=nv, num_core_orbs=nc)
-    phi_f = device.spmm(Dout, X)
-    Hf = device.build_csr(device.HAM_I, ff, hop_i, coul_i, num_val_orbs=nv)
-    r = device.krylov(Hf, phi_f, cfg["nkryl"])
+    with trace.phase("rixs: D_out^+ x"):
+        Dout = device.build_csr(device.TRANS_F, ff, tr_f, right=fn, num_val_orbs=nv, num_core_orbs=nc)
+        phi_f = device.spmm(Dout, X)
+    with trace.phase("rixs: build H_f"):
+        Hf = device.build_csr(device.HAM_I, ff, hop_i, coul_i, num_val_orbs=nv)
+    with trace.phase("rixs: Krylov"):
+        r = device.krylov(Hf, phi_f, cfg["nkryl"])
     _write_poles("rixs_poles", r, evals)
 
 
@@ -174,9 +186,10 @@ def opavg_fsolver(comm=0, my_id=0, num_procs=1):
     hop = edxio.read_hopping(_path("hopping_i.in"))
     coul = edxio.read_coulomb(_path("coulomb_i.in"))
     fi = device.basis_from_states(edxio.read_fock(_path("fock_i.in")))
-    O = device.build_csr(device.HAM_I, fi, hop, coul, num_val_orbs=cfg["num_val_orbs"])
     evals, g = _read_gs(cfg["num_gs"], fi.ndim)
-    G = torch.from_numpy(g).cuda()
-    OG = device.spmm(O, G)
-    avg = (G.conj() * OG).sum(dim=0).cpu().numpy()
+    with trace.phase("opavg: build O, <v|O|v>"):
+        O = device.build_csr(device.HAM_I, fi, hop, coul, num_val_orbs=cfg["num_val_orbs"])
+        G = torch.from_numpy(g).cuda()
+        OG = device.spmm(O, G)
+        avg = (G.conj() * OG).sum(dim=0).cpu().numpy()
     edxio.write_opavg(_path("opavg.dat"), evals, avg)

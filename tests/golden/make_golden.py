@@ -448,7 +448,16 @@ def callers_2v1c(ed, out_dir):
                              pol_type=[("linear", 0.0)], num_gs=1, nkryl=100, **geo)
             ed.xas_2v1c_fort(comm, shells, om, gamma_c=0.3, v_tot_noccu=10, trans_to_which=1,
                              pol_type=[("linear", 0.3)], num_gs=1, nkryl=100, **geo)
-            ed.rixs_2v1c_fort(comm, shells, np.array([1.0, 3.0]), np.linspace(-0.5, 4.0, 5), gamma_c=0.5,
+            # incident energies near the edge, where the RIXS amplitudes are large
+            from oracle import pyoracle as orc
+            e_i = np.linalg.eigvalsh(orc.build_csr(
+                "ham_i", orc.read_fock("fock_i.in"), orc.read_terms("hopping_i.in", 2),
+                orc.read_terms("coulomb_i.in", 4), num_val_orbs=12).dense())[0]
+            e_n = np.linalg.eigvalsh(orc.build_csr(
+                "ham_n", orc.read_fock("fock_n.in"), orc.read_terms("hopping_n.in", 2),
+                orc.read_terms("coulomb_n.in", 4), num_val_orbs=12, num_core_orbs=2).dense())[0]
+            ominc = round(float(e_n - e_i), 4) + np.array([0.5, 2.0])
+            ed.rixs_2v1c_fort(comm, shells, ominc, np.linspace(-0.5, 4.0, 5), gamma_c=0.5,
                               gamma_f=0.1, v_tot_noccu=10, trans_to_which=2, thout=1.0,
                               pol_type=[("linear", 0.0, "linear", np.pi / 2)], num_gs=1, nkryl=100,
                               linsys_max=500, linsys_tol=1e-12, **geo)

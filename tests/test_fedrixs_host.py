@@ -137,3 +137,61 @@ def test_drop_in_host_logic_reproduces_kramers_heisenberg(host_device, tmp_path,
     assert names[:3] == ["ed: build H_i", "ed: eigenpairs", "ed: density matrix"]
     assert names.count("xas: Krylov") == 2 and names.count("rixs: MINRES") == 2
     assert names[-1] == "opavg: build O, <v|O|v>" and all(r["ok"] for r in trace.records)
+
+
+def test_drop_in_host_logic_on_two_valence_shell_files(host_device, tmp_path, monkeypatch):
+    """The same on the files of the reference's 2v1c callers (t2g + p shells, an s core of two
+    orbitals, a quadrupolar operator; tests/golden/callers_2v1c), against the exact spectra of
+    the matrices the reference's two_fermion / four_fermion build from them."""
+    G = os.path.join(os.path.dirname(KH), "callers_2v1c")
+    with np.load(os.path.join(G, "dense.npz")) as z:
+        d = {k: z[k] for k in z.files}
+    M = {}
+    for key in d:
+        if key.endswith("_shape"):
+            name = key[:-6]
+            M[name] = np.zeros(tuple(d[key]), dtype=complex)
+            M[name][d[name + "_row"], d[name + "_col"]] = d[name + "_val"]
+
+    def exact(H, phi, e0, om, gam):
+        ev, U = np.linalg.eigh(H)
+        w2 = np.abs(U.conj().T @ phi) ** 2
+        return -np.imag((w2[None, :] / (om[:, None] + 1j * gam + e0 - ev[None, :])).sum(axis=1)) / np.pi
+
+    def workdir(name, e0=None, g0=None):
+        w = tmp_path / name
+        w.mkdir()
+        for src in {os.path.join(G, "ed_00"), os.path.join(G, name)}:
+            if os.path.isdir(src):
+                for fn in os.listdir(src):
+                    shutil.copy(os.path.join(src, fn), w / fn)
+        if g0 is not None:
+            edxio.write_eigvec(str(w / "eigvec.1"), e0, g0)
+        monkeypatch.chdir(w)
+        return w
+
+    w = workdir("ed_00")
+    fedrixs.ed_fsolver(0, 0, 1)
+    e, v = np.linalg.eigh(M["H_i"])
+    assert np.allclose(np.loadtxt(w / "eigvals.dat", ndmin=2)[:, 1], e[:2], atol=1e-9)
+    om = np.linalg.eigvalsh(M["H_n"])[0] - e[0] + np.linspace(-3.0, 12.0, 151)
+    for name in ("xas_01", "xas_02"):
+        w = workdir(name, e[0], v[:, 0])
+        fedrixs.xas_fsolver(0, 0, 1)
+        spec = orc.spectra_from_poles(edxio.read_poles([str(w / "xas_poles.1")]), om, 0.3, 1.0)
+        ref = exact(M["H_n"], M[f"D_{name}"] @ v[:, 0], e[0], om, 0.3)
+        assert np.abs(spec - ref).max() <= 1e-7 * np.abs(ref).max()
+    eloss = np.linspace(-0.5, 6.0, 66)
+    for name in ("rixs_03", "rixs_04"):
+        w = workdir(name, e[0], v[:, 0])
+        cfg = edxio.read_config(str(w / "config.in"))
+        fedrixs.rixs_fsolver(0, 0, 1)
+        poles = edxio.read_poles([str(w / "rixs_poles.1")])
+        spec = orc.spectra_from_poles(poles, eloss, 0.1, 1.0)
+        z = cfg["omega_in"] + e[0] + 1j * cfg["gamma_in"]
+        x = np.linalg.solve(z * np.eye(len(M["H_n"])) - M["H_n"], M[f"D_in_{name}"] @ v[:, 0])
+        ref = exact(M["H_i"], M[f"D_out_{name}"] @ x, e[0], eloss, 0.1)
+        # off resonance the norm is small, and the file carries it to 10 decimals
+        # (src/io.f90:532-537): a relative error of up to 5e-11 / norm comes from the format
+        tol = 1e-7 + 5e-11 / poles["norm"][0]
+        assert np.abs(spec - ref).max() <= tol * np.abs(ref).max()

@@ -111,7 +111,8 @@ def test_2v1c_xas_and_rixs_match_kramers_heisenberg(dense, tmp_path):
     e, v = np.linalg.eigh(dense["H_i"])
     assert e[1] - e[0] > 1e-3          # a non-degenerate ground state
     e0, g0 = float(e[0]), v[:, 0]
-    om = np.linspace(-3.0, 12.0, 301)
+    edge = np.linalg.eigvalsh(dense["H_n"])[0] - e0
+    om = edge + np.linspace(-3.0, 12.0, 301)
     for name in ("xas_01", "xas_02"):
         (a, b, nrm, neff, eg), = odrv.xas(_workdir(tmp_path, name, e0, g0))
         poles = {"npoles": [neff], "eigval": [eg], "norm": [nrm], "alpha": [a], "beta": [b]}

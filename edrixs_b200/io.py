@@ -91,22 +91,39 @@ def read_config(path="config.in"):
     return cfg
 
 
+def _count(path, line):
+    try:
+        n = int(line.split()[0])
+    except (ValueError, IndexError):
+        raise EdxInputError(f"{path}: the first line must hold the count, got {line.strip()!r}") from None
+    if n < 0:
+        raise EdxInputError(f"{path}: negative count {n}")
+    return n
+
+
 def _read_counted(path, nidx):
+    """Line 1 = count, then `nidx` 1-based orbital indices and a complex value per term
+    (src/io.f90:86-152; written by edrixs/iostream.py:165-236)."""
     _need(path)
     with open(path) as f:
         first = f.readline()
         if not first.strip():
             raise EdxInputError(f"{path}: empty file")
-        n = int(first.split()[0])
+        n = _count(path, first)
         data = f.read().split()
     need = n * (nidx + 2)
     if len(data) < need:
         raise EdxInputError(f"{path}: expected {n} terms, file is short")
     arr = np.array(data[:need], dtype=object).reshape(n, nidx + 2)
-    idx = arr[:, :nidx].astype(np.int64).astype(np.int32)
-    vals = np.array([_fortran_float(x) for x in arr[:, nidx:].ravel()], dtype=np.float64)
+    try:
+        idx = np.array([int(x) for x in arr[:, :nidx].ravel()], dtype=np.int64).reshape(n, nidx)
+        vals = np.array([_fortran_float(x) for x in arr[:, nidx:].ravel()], dtype=np.float64)
+    except ValueError as e:
+        raise EdxInputError(f"{path}: malformed term ({e})") from None
+    if n and (idx.min() < 1 or idx.max() > 64):
+        raise EdxInputError(f"{path}: orbital indices must lie in 1..64 (1-based)")
     val = vals.reshape(n, 2) @ np.array([1.0, 1j])
-    return idx, val.astype(np.complex128)
+    return idx.astype(np.int32), val.astype(np.complex128)
 
 
 def read_hopping(path):
@@ -123,11 +140,21 @@ def read_fock(path):
     """Fock basis file -> uint64 array (reference keeps int64; values are < 2^63)."""
     _need(path)
     with open(path) as f:
-        n = int(f.readline().split()[0])
+        n = _count(path, f.readline())
         data = f.read().split()
     if len(data) < n:
         raise EdxInputError(f"{path}: expected {n} states, file is short")
-    return np.array(data[:n], dtype=np.int64).astype(np.uint64)
+    try:
+        states = np.array(data[:n], dtype=np.int64)
+    except (ValueError, OverflowError) as e:
+        raise EdxInputError(f"{path}: malformed state ({e})") from None
+    # the writer sorts (edrixs/fock_basis.py:444) and the column search needs it
+    # (src/utils.f90:2-40): an unsorted or repeated list would give wrong matrices silently
+    if n > 1 and not np.all(np.diff(states) > 0):
+        raise EdxInputError(f"{path}: states are not strictly ascending")
+    if n and states[0] < 0:
+        raise EdxInputError(f"{path}: negative state")
+    return states.astype(np.uint64)
 
 
 def read_eigvec(path, n=None):

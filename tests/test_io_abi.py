@@ -39,6 +39,34 @@ def test_missing_file_raises(tmp_path):
         edxio.read_hopping(str(tmp_path / "hopping_i.in"))
 
 
+@pytest.mark.parametrize("text,msg", [
+    ("abc\n1 1 0.5 0\n", "count"), ("-2\n1 1 0.5 0\n", "negative count"),
+    ("2\n1 1 0.5 0\n", "short"), ("1\nx 1 0.5 0\n", "malformed term"),
+    ("1\n1.5 1 0.5 0\n", "malformed term"), ("1\n1 1 zz 0\n", "malformed term"),
+    ("1\n0 1 0.5 0\n", "1..64"),
+])
+def test_malformed_term_files_raise_input_errors(tmp_path, text, msg):
+    """A malformed hopping / Coulomb / transition file fails with EdxInputError naming the
+    file, where the reference STOPs (src/io.f90:86-89)."""
+    p = tmp_path / "hopping_i.in"
+    p.write_text(text)
+    with pytest.raises(edxio.EdxInputError, match=msg):
+        edxio.read_hopping(str(p))
+
+
+@pytest.mark.parametrize("text,msg", [
+    ("3\n1\n2\n", "short"), ("2\n3\n1\n", "ascending"), ("2\n1\n1\n", "ascending"),
+    ("2\n1\nx\n", "malformed state"), ("x\n1\n", "count"),
+])
+def test_malformed_fock_files_raise_input_errors(tmp_path, text, msg):
+    """The reference's writer sorts the basis (edrixs/fock_basis.py:444) and its column search
+    relies on it (src/utils.f90:2-40), so an unsorted or repeated list is rejected."""
+    p = tmp_path / "fock_i.in"
+    p.write_text(text)
+    with pytest.raises(edxio.EdxInputError, match=msg):
+        edxio.read_fock(str(p))
+
+
 def test_reference_caller_files_parse(golden_dir):
     d = os.path.join(golden_dir, "siam_callers", "rixs_2")
     cfg = edxio.read_config(os.path.join(d, "config.in"))

@@ -69,8 +69,12 @@ def fock_unrank(norb, nelec):
 
 def basis_from_states(states):
     """Wrap a sorted state list (e.g. read from fock_*.in); detects the full-sector case."""
-    require_cuda()
     arr = np.asarray(states, dtype=np.uint64)
+    if len(arr) > 1 and not np.all(arr[1:] > arr[:-1]):
+        # the column search (src/utils.f90:2-40) needs ascending states; unsorted or repeated
+        # ones would give wrong matrices without an error
+        raise ValueError("basis_from_states: states must be strictly ascending")
+    require_cuda()
     t = torch.from_numpy(arr.view(np.int64)).to("cuda")
     b = Basis(t)
     if len(arr) == 0:

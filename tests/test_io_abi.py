@@ -299,3 +299,11 @@ def test_product_package_never_imports_the_oracle():
                 if any(n == "oracle" or n.startswith("oracle.") for n in names):
                     offenders.append(os.path.relpath(path, ROOT))
     assert not offenders, offenders
+
+
+def test_device_basis_rejects_unsorted_states():
+    """Checked on the host before any device work: the column search needs ascending states."""
+    from edrixs_b200 import device
+    for bad in ([3, 1, 2], [1, 1]):
+        with pytest.raises(ValueError, match="ascending"):
+            device.basis_from_states(np.array(bad, dtype=np.uint64))

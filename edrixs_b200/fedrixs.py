@@ -51,6 +51,10 @@ def ed_core(cfg, H):
     ed_solver = cfg["ed_solver"]
     if ndim < cfg["min_ndim"]:
         ed_solver = 0
+    elif ed_solver not in (1, 2):
+        # the reference has no branch for other values and writes unset eigenvalues
+        # (src/ed_driver.f90:127-171)
+        raise edxio.EdxInputError(f"config.in: ed_solver must be 0, 1 or 2 (got {ed_solver})")
     neval = min(cfg["neval"], ndim)
     nvector = min(cfg["nvector"], ndim)
     if ed_solver == 0:

@@ -78,14 +78,23 @@ def read_config(path="config.in"):
     for key, val in re.findall(r"([A-Za-z_][A-Za-z0-9_]*)\s*=\s*([^,\n]+)", body):
         k = key.lower()
         v = val.strip().rstrip(",").strip()
-        if k in _INT_KEYS:
-            cfg[k] = int(float(v.lower().replace("d", "e")))
-        elif k in _FLOAT_KEYS:
-            cfg[k] = _fortran_float(v)
-        elif k in _BOOL_KEYS:
-            cfg[k] = _fortran_bool(v)
-        else:
-            raise EdxInputError(f"config.in: unknown namelist key {key!r}")
+        try:
+            if k in _INT_KEYS:
+                x = float(v.lower().replace("d", "e"))
+                if not x.is_integer():
+                    raise ValueError(f"{v!r} is not an integer")
+                cfg[k] = int(x)
+            elif k in _FLOAT_KEYS:
+                cfg[k] = _fortran_float(v)
+            elif k in _BOOL_KEYS:
+                cfg[k] = _fortran_bool(v)
+            else:
+                raise EdxInputError(f"config.in: unknown namelist key {key!r}")
+        except ValueError as e:
+            raise EdxInputError(f"config.in: bad value for {key}: {e}") from None
+    for k in _INT_KEYS:
+        if cfg[k] is not None and cfg[k] < 0:
+            raise EdxInputError(f"config.in: {k} must not be negative (got {cfg[k]})")
     if cfg["ncv"] is None:  # io.f90:27 ncv = neval + 2 (evaluated after neval's default)
         cfg["ncv"] = CONFIG_DEFAULTS["neval"] + 2
     return cfg
@@ -165,15 +174,19 @@ def read_eigvec(path, n=None):
     pos = 0
     recs = []
     while pos < len(raw):
+        if pos + 4 > len(raw):
+            raise EdxInputError(f"{path}: truncated Fortran record")
         (ln,) = struct.unpack_from("<i", raw, pos)
         pos += 4
+        if ln < 0 or pos + ln + 4 > len(raw):
+            raise EdxInputError(f"{path}: truncated Fortran record")
         recs.append(raw[pos:pos + ln])
         pos += ln
         (ln2,) = struct.unpack_from("<i", raw, pos)
         pos += 4
         if ln2 != ln:
             raise EdxInputError(f"{path}: corrupt Fortran record markers")
-    if len(recs) < 2 or len(recs[0]) != 8:
+    if len(recs) < 2 or len(recs[0]) != 8 or len(recs[1]) % 16:
         raise EdxInputError(f"{path}: not an eigvec file")
     e = struct.unpack("<d", recs[0])[0]
     v = np.frombuffer(recs[1], dtype=np.complex128).copy()

@@ -307,3 +307,34 @@ def test_device_basis_rejects_unsorted_states():
     for bad in ([3, 1, 2], [1, 1]):
         with pytest.raises(ValueError, match="ascending"):
             device.basis_from_states(np.array(bad, dtype=np.uint64))
+
+
+@pytest.mark.parametrize("body,msg", [
+    ("neval=abc", "bad value for neval"), ("eigval_tol=x", "bad value for eigval_tol"),
+    ("neval=2.5", "not an integer"), ("num_val_orbs=-3", "must not be negative"),
+])
+def test_config_bad_values_raise_input_errors(tmp_path, body, msg):
+    p = tmp_path / "config.in"
+    p.write_text(f"&control\n{body}\n&end\n")
+    with pytest.raises(edxio.EdxInputError, match=msg):
+        edxio.read_config(str(p))
+
+
+def test_truncated_eigvec_raises_input_error(tmp_path):
+    p = tmp_path / "eigvec.1"
+    edxio.write_eigvec(str(p), -1.0, np.ones(4, dtype=np.complex128))
+    raw = p.read_bytes()
+    for cut in (6, 20, len(raw) - 2):
+        p.write_bytes(raw[:cut])
+        with pytest.raises(edxio.EdxInputError):
+            edxio.read_eigvec(str(p), 4)
+
+
+def test_unknown_ed_solver_is_refused_above_min_ndim():
+    """src/ed_driver.f90:127-171 has branches for ed_solver 0, 1 and 2 only (below min_ndim
+    it switches to 0 itself)."""
+    from types import SimpleNamespace
+    from edrixs_b200 import fedrixs
+    cfg = dict(edxio.CONFIG_DEFAULTS, ed_solver=3, min_ndim=1000, ncv=3)
+    with pytest.raises(edxio.EdxInputError, match="ed_solver"):
+        fedrixs.ed_core(cfg, SimpleNamespace(nrows=5000))

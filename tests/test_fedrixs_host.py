@@ -195,3 +195,17 @@ def test_drop_in_host_logic_on_two_valence_shell_files(host_device, tmp_path, mo
         # (src/io.f90:532-537): a relative error of up to 5e-11 / norm comes from the format
         tol = 1e-7 + 5e-11 / poles["norm"][0]
         assert np.abs(spec - ref).max() <= tol * np.abs(ref).max()
+
+
+def test_command_line_entry_points(host_device, tmp_path, monkeypatch, capsys):
+    """`python -m edrixs_b200.scripts ed|xas|rixs|opavg` (the ed.x ... opavg.x of the reference,
+    setup.py:101-108) run the drop-in solvers in the working directory; a nonzero RANK runs
+    nothing; a bad command prints the usage and returns 2."""
+    from edrixs_b200 import scripts
+    d = _workdir(tmp_path, "ed_00")
+    monkeypatch.chdir(d)
+    monkeypatch.setenv("RANK", "1")
+    assert scripts.main(["ed"]) == 0 and not (d / "eigvals.dat").exists()
+    monkeypatch.setenv("RANK", "0")
+    assert scripts.main(["ed"]) == 0 and (d / "eigvals.dat").exists() and (d / "denmat.dat").exists()
+    assert scripts.main(["bogus"]) == 2 and "usage" in capsys.readouterr().err

@@ -219,13 +219,21 @@ class Server:
             fut.set_exception(MemoryError(f"request {req.id} needs more than the HBM budget"))
             return fut
         with self.cv:
+            if self.stop_flag:
+                fut.set_exception(RuntimeError(f"request {req.id}: the server is shut down"))
+                return fut
             self.waiting.append((req, fut))
             self.cv.notify_all()
         return fut
 
     def shutdown(self):
+        """Stop taking work.  Requests still waiting are cancelled (their futures raise
+        CancelledError); solves already running finish first."""
         with self.cv:
             self.stop_flag = True
+            for _, fut in self.waiting:
+                fut.cancel()
+            self.waiting = []
             self.cv.notify_all()
         for _ in self.threads:
             self.jobs.put(None)

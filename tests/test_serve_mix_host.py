@@ -3,6 +3,7 @@ import math
 import types
 
 import numpy as np
+import pytest
 
 
 def test_serve_mix_is_seeded_and_in_range():
@@ -148,3 +149,19 @@ def test_cancelled_requests_leave_the_queue_and_the_coalesced_solve():
     assert groups == [[first.id], [b.id]]
     assert fa.cancelled() and fc.cancelled() and fb.running()
     assert srv.waiting == [] and srv.free_workers == 1 and srv.inflight_bytes == 0
+
+
+def test_shutdown_cancels_waiting_requests_and_refuses_new_ones():
+    """After shutdown no future is left pending for ever: waiting requests are cancelled and
+    later submissions fail at once.  (Server not started: no GPU.)"""
+    from concurrent.futures import CancelledError
+    from edrixs_b200.serve import ModelSpec, Request, Server
+    srv = Server(hbm_budget=1e12, workers=1)
+    f1 = srv.submit(Request("ed", ModelSpec(4, 7, 1)))
+    srv.shutdown()
+    with pytest.raises(CancelledError):
+        f1.result(timeout=1)
+    f2 = srv.submit(Request("ed", ModelSpec(4, 7, 2)))
+    with pytest.raises(RuntimeError, match="shut down"):
+        f2.result(timeout=1)
+    assert srv.waiting == []

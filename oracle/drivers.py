@@ -32,8 +32,11 @@ def _cfg(path):
     return cfg
 
 
-def ed(directory):
-    """-> eigvals (neval), eigvecs (n, nvector), H csr, fock, cfg"""
+def ed(directory, follow_ed_solver=False):
+    """-> eigvals (neval), eigvecs (n, nvector), H csr, fock, cfg.  By default the eigenpairs
+    are those of ed_solver 0 / 2 (dense or ARPACK).  With follow_ed_solver, ed_solver = 1 at
+    or above min_ndim runs the step-for-step plain Lanczos of lanczos.f90:6-167 instead, as
+    ed_driver.f90:154-158 does (seeded; lowest distinct levels on degenerate spectra)."""
     p = lambda f: os.path.join(directory, f)  # noqa: E731
     cfg = _cfg(p("config.in"))
     fock = orc.read_fock(p("fock_i.in"))
@@ -41,6 +44,9 @@ def ed(directory):
                       num_val_orbs=cfg["num_val_orbs"])
     neval = min(cfg["neval"], len(fock))
     nvec = min(cfg["nvector"], len(fock))
+    if follow_ed_solver and cfg["ed_solver"] == 1 and len(fock) >= cfg["min_ndim"]:
+        e, v, _ = orc.lanczos_eigs(H, neval, cfg["maxiter"], cfg["eigval_tol"], nvec=nvec)
+        return e, v, H, fock, cfg
     e, v = orc.ed_eigs(H, max(neval, nvec))
     return e[:neval], v[:, :nvec], H, fock, cfg
 

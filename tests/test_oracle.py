@@ -275,3 +275,20 @@ def test_opavg_file_format(tmp_path):
     lines = open(p).read().splitlines()
     assert lines[0] == "    1" + "{:20.10f}".format(-12.5) + "{:20.10f}".format(2.25) + "{:20.10f}".format(-0.0)
     assert len(lines[1]) == 65 and lines[1].startswith("    2")
+
+
+def test_oracle_ed_driver_follows_ed_solver_1(golden_dir, tmp_path):
+    """drivers.ed(follow_ed_solver=True) on the known-answer files with ed_solver = 1 and
+    min_ndim below the dimension: the plain Lanczos path of ed_driver.f90:154-158."""
+    import shutil
+    from oracle import drivers as odrv
+    d = tmp_path / "ka"
+    shutil.copytree(os.path.join(golden_dir, "known_answer"), d)
+    (d / "config.in").write_text("&control\ned_solver=1\nnum_val_orbs=20\nneval=3\nnvector=2\n"
+                                 "maxiter=500\neigval_tol=1e-10\nmin_ndim=10\n&end\n")
+    expected = np.loadtxt(d / "expected_eigvals.txt")
+    levels = expected[np.r_[True, np.diff(expected) > 1e-8]]
+    e, v, H, fock, cfg = odrv.ed(str(d), follow_ed_solver=True)
+    assert np.abs(e - levels[:3]).max() < 1e-10 and v.shape == (45, 2)
+    e0, _, _, _, _ = odrv.ed(str(d))
+    assert np.abs(e0 - expected[:3]).max() < 1e-10    # dense: the 9-fold level three times

@@ -98,6 +98,9 @@ class Resident:
         return b
 
     def ensure(self, need_n=False, ngs=1):
+        """Build what is missing and return a snapshot (gs_e, gs_v) of the ground states.
+        A later request for more ground states replaces gs_e and gs_v; a solve uses only its
+        own snapshot, so it never mixes the eigenvalues of one set with the vectors of another."""
         with self.lock:
             s = self.spec
             if self.model is None:
@@ -123,6 +126,7 @@ class Resident:
             # the resident is shared with other workers' streams: finish building it here
             torch.cuda.current_stream().synchronize()
             self.last_used = time.monotonic()
+            return self.gs_e, self.gs_v
 
     def op(self, kind, pol):
         key = (kind, pol)
@@ -302,7 +306,9 @@ class Server:
                 res.busy += 1
                 self.inflight_bytes += need
                 self.free_workers -= 1
-            self.jobs.put((group, res, need))
+                # queued while the lock is held: shutdown() takes the lock before it queues
+                # the workers' stop markers, so a picked job always reaches a worker first
+                self.jobs.put((group, res, need))
 
     def _work(self, idx):
         stream = torch.cuda.Stream()
@@ -337,20 +343,23 @@ class Server:
     def _run(self, group, res: Resident):
         req = group[0][0]
         if req.kind == "ed":
-            res.ensure(False, req.ngs)
-            return [{"eigvals": res.gs_e[:r.ngs].copy()} for r, _ in group]
+            gs_e, _ = res.ensure(False, req.ngs)
+            return [{"eigvals": gs_e[:r.ngs].copy()} for r, _ in group]
         G = max(r.ngs for r, _ in group)
-        res.ensure(True, G)
+        gs_e, gs_v = res.ensure(True, G)
+        # this stream reads the snapshot: if another request replaces it meanwhile, the
+        # caching allocator keeps its memory until the work queued here has finished
+        gs_v.record_stream(torch.cuda.current_stream())
         if req.kind == "xas":
-            return self._xas_group(group, res)
+            return self._xas_group(group, res, gs_e, gs_v)
         # union of incident energies (absolute) and polarisations over the coalesced requests
         oms = [np.asarray(r.omegas, dtype=np.float64) + res.edge for r, _ in group]
         allw = np.unique(np.concatenate(oms))
         pins = sorted(set(siam_pol_in(p) for r, _ in group for p in r.pols))
         pouts = sorted(set(siam_pol_out(p) for r, _ in group for p in r.pols))
         P = rixs.RixsProblem(Hn=res.Hn, Hf=res.Hi, Din=[res.op("in", p) for p in pins],
-                             Dout=[res.op("out", p) for p in pouts], gs_e=res.gs_e[:G],
-                             gs_v=res.gs_v[:, :G].contiguous(),
+                             Dout=[res.op("out", p) for p in pouts], gs_e=gs_e[:G],
+                             gs_v=gs_v[:, :G].contiguous(),
                              packed={k: v for k, v in (("hf", res.packed.get("hi")), ("hn", res.packed.get("hn")))
                                      if v is not None})
         out = rixs.rixs_spectra(P, allw, req.gamma_c, req.eloss, req.gamma_f, nkryl=req.nkryl,
@@ -360,19 +369,20 @@ class Server:
         for (r, _), om in zip(group, oms):
             idx = np.searchsorted(allw, om)
             cols = [pins.index(siam_pol_in(p)) * len(pouts) + pouts.index(siam_pol_out(p)) for p in r.pols]
-            w = rixs.boltz(res.gs_e[:r.ngs], r.temperature)  # this request's own ground states
+            w = rixs.boltz(gs_e[:r.ngs], r.temperature)  # this request's own ground states
             spec = np.einsum("weng,g->wen", out.spectra_gs[idx][:, :, cols, :r.ngs], w)
             results.append({"omegas": om, "spectra": spec, "coalesced": len(group), "minres_iters": out.iters})
         return results
 
-    def _xas_group(self, group, res: Resident):
+    def _xas_group(self, group, res: Resident, gs_e, gs_v):
         """XAS of every request in the group from one Krylov launch: the start vectors
         D_xas(pol)|g> of all of them side by side (build_krylov_mp per column, as the
-        reference runs them one by one), then each request's continued fraction."""
+        reference runs them one by one), then each request's continued fraction.  gs_e, gs_v:
+        the ground-state snapshot this solve took."""
         phis, spans = [], []
         c0 = 0
         for r, _ in group:
-            phis.append(device.spmm(res.op("xas", r.pols[0]), res.gs_v[:, :r.ngs].contiguous()))
+            phis.append(device.spmm(res.op("xas", r.pols[0]), gs_v[:, :r.ngs].contiguous()))
             spans.append((c0, c0 + r.ngs))
             c0 += r.ngs
         phi = torch.cat(phis, dim=1).contiguous()
@@ -381,9 +391,9 @@ class Server:
         norm = kr.norm.cpu().numpy()
         out = []
         for (r, _), (a, b) in zip(group, spans):
-            w = rixs.boltz(res.gs_e[:r.ngs], r.temperature)
+            w = rixs.boltz(gs_e[:r.ngs], r.temperature)
             grid = np.asarray(r.eloss, dtype=np.float64) + res.edge
-            spec = device.cf_spectrum(kr.neff[a:b], kr.alpha[a:b], kr.beta[a:b], res.gs_e[:r.ngs], norm[a:b], w,
+            spec = device.cf_spectrum(kr.neff[a:b], kr.alpha[a:b], kr.beta[a:b], gs_e[:r.ngs], norm[a:b], w,
                                       grid, np.full(len(grid), r.gamma_c))
             out.append({"grid": grid, "spectrum": spec.cpu().numpy(), "coalesced": len(group)})
         return out

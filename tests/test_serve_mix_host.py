@@ -165,3 +165,54 @@ def test_shutdown_cancels_waiting_requests_and_refuses_new_ones():
     with pytest.raises(RuntimeError, match="shut down"):
         f2.result(timeout=1)
     assert srv.waiting == []
+
+
+def test_shutdown_between_pick_and_queue_leaves_no_future_pending():
+    """shutdown() that runs while the scheduler hands a picked request to the job queue must
+    not strand it: the job is queued ahead of the workers' stop markers, so a worker still
+    takes it and its future completes.  The job queue here stalls the scheduler inside its
+    put and starts shutdown() meanwhile.  (No GPU: a fake worker takes the jobs.)"""
+    import queue
+    import threading
+    import time
+    from edrixs_b200.serve import ModelSpec, Request, Server
+    srv = Server(hbm_budget=1e12, workers=1)
+    stalled = []
+
+    class StallingQueue(queue.Queue):
+        def put(self, item, *a, **kw):
+            if item is not None and not stalled:
+                t = threading.Thread(target=srv.shutdown, daemon=True)
+                stalled.append(t)
+                t.start()
+                time.sleep(0.3)  # the scheduler is descheduled here; shutdown() runs meanwhile
+            super().put(item, *a, **kw)
+
+    srv.jobs = StallingQueue()
+
+    def fake_worker():
+        while True:
+            job = srv.jobs.get()
+            if job is None:
+                return
+            group, res, need = job
+            for r, f in group:
+                f.set_result(r.id)
+            with srv.cv:
+                res.busy -= 1
+                srv.inflight_bytes -= need
+                srv.free_workers += 1
+                srv.cv.notify_all()
+
+    worker = threading.Thread(target=fake_worker, daemon=True)
+    worker.start()
+    srv.threads.append(worker)
+    sched = threading.Thread(target=srv._schedule, daemon=True)
+    sched.start()
+    req = Request("ed", ModelSpec(4, 7, 1))
+    fut = srv.submit(req)
+    assert fut.result(timeout=5) == req.id
+    stalled[0].join(timeout=5)
+    worker.join(timeout=5)
+    assert not worker.is_alive() and srv.stop_flag
+    assert srv.free_workers == 1 and srv.inflight_bytes == 0

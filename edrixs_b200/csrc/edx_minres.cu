@@ -442,26 +442,18 @@ namespace edx {
 static __device__ __align__(256) double2
     g_denmat_scratch[(size_t)EDX_DENMAT_STATIC_CHUNKS * EDX_DENMAT_STATIC_MAX_ENTRIES];
 
-static std::mutex g_denmat_scratch_mu;
-static double2* g_denmat_scratch_ptr[EDX_MAX_DEVICES];
-
 // Device address of g_denmat_scratch for the current device.  In host code the symbol's
-// name is only a host-side stand-in, so the address is looked up once per device, with that
-// device current, and cached.
+// name is only a host-side stand-in, so the address is looked up with the device current.
+// It is looked up on every call rather than cached: after cudaDeviceReset the library's
+// device code is loaded again, possibly at another address, and a cached pointer would be
+// stale.  Once the module is loaded the lookup is a cheap host-side query.
 static int denmat_scratch_address(double2** out) {
-    int dev = 0;
-    EDX_CUDA(cudaGetDevice(&dev));
-    EDX_REQUIRE(dev >= 0 && dev < EDX_MAX_DEVICES, "edx_denmat_static: device ordinal %d out of range", dev);
-    std::lock_guard<std::mutex> lk(g_denmat_scratch_mu);
-    if (g_denmat_scratch_ptr[dev] == nullptr) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_denmat_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return fail(EDX_ERR_CUDA, "edx_denmat_static: cudaGetSymbolAddress of the scratch array failed: %s",
-                        cudaGetErrorString(e));
-        g_denmat_scratch_ptr[dev] = static_cast<double2*>(p);
-    }
-    *out = g_denmat_scratch_ptr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_denmat_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        return fail(EDX_ERR_CUDA, "edx_denmat_static: cudaGetSymbolAddress of the scratch array failed: %s",
+                    cudaGetErrorString(e));
+    *out = static_cast<double2*>(p);
     return EDX_OK;
 }
 

@@ -374,10 +374,11 @@ int edx_denmat(const uint64_t* d_fock, int64_t n, int search_norb, int search_ne
  * in a fixed file-scope device array of EDX_DENMAT_STATIC_CHUNKS x
  * EDX_DENMAT_STATIC_MAX_ENTRIES complex128 values (4 MiB) that every GPU loading the library
  * holds until the process exits.  Limit: nvec * nv * nv <= EDX_DENMAT_STATIC_MAX_ENTRIES,
- * otherwise EDX_ERR_INVALID.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) with that device current; make that first call before any
- * stream capture.  All calls share the one array: calls that overlap on the GPU (for
- * example on two streams) race and must be serialised by the caller.  Allocates nothing. */
+ * otherwise EDX_ERR_INVALID.  Every call looks up the array's device address
+ * (cudaGetSymbolAddress) with the calling device current, so the address stays right after
+ * a cudaDeviceReset; the first call on a device may load the library's device code, so make
+ * it before any stream capture.  All calls share the one array: calls that overlap on the GPU
+ * (for example on two streams) race and must be serialised by the caller.  Allocates nothing. */
 #define EDX_DENMAT_STATIC_CHUNKS 64
 #define EDX_DENMAT_STATIC_MAX_ENTRIES 4096
 #define EDX_MAX_DEVICES 64

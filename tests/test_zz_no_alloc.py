@@ -50,10 +50,53 @@ def test_denmat_static_matches_workspace_version(cuda):
         assert rc == 0, L.edx_last_error()
         got = out.cpu().numpy()
         assert np.all(np.isfinite(got))
-        # same kernel, different number of row chunks: equal up to summation order
+        # same kernel; at this size both entry points use the same 4 row chunks
         assert np.abs(got - want).max() <= 1e-12 * max(1.0, np.abs(want).max()), f"call {call}"
         tr = np.trace(got, axis1=1, axis2=2).real
         assert np.allclose(tr, 5.0, atol=1e-10)  # N electrons in every eigenvector
+
+
+def _both(L, basis, vecs, nv, nvec):
+    """edx_denmat (with a workspace) and edx_denmat_static on the same input."""
+    import torch
+    from edrixs_b200.device import _ptr, _stream, _work
+    n = basis.ndim
+    ref = torch.zeros((nvec, nv, nv), dtype=torch.complex128, device="cuda")
+    ws = ctypes.c_size_t(0)
+    assert L.edx_denmat_workspace(n, nv, nvec, ctypes.byref(ws)) == 0
+    w = _work(ws.value)
+    assert L.edx_denmat(_ptr(basis.states), n, basis.norb, basis.nelec, nv, nvec, _ptr(vecs), _ptr(ref), _ptr(w),
+                        ws.value, _stream()) == 0
+    outs = []
+    for _ in range(2):
+        out = torch.full((nvec, nv, nv), complex(np.nan, np.nan), dtype=torch.complex128, device="cuda")
+        rc = L.edx_denmat_static(_ptr(basis.states), n, basis.norb, basis.nelec, nv, nvec, _ptr(vecs), _ptr(out),
+                                 _stream())
+        assert rc == 0, L.edx_last_error()
+        outs.append(out.cpu().numpy())
+    return ref.cpu().numpy(), outs
+
+
+def test_denmat_static_above_the_chunk_cap(cuda):
+    """38,760 rows (20 orbitals, 6 electrons): edx_denmat splits them into more than the 64
+    row chunks the static array holds, so edx_denmat_static takes the clamped path (64 longer
+    chunks).  The two differ only in summation order."""
+    import torch
+    from edrixs_b200 import _lib, device
+    L = _lib.load()
+    nv, nelec, nvec = 20, 6, 3
+    basis = device.fock_unrank(nv, nelec)
+    assert basis.ndim > 64 * 256
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    v = torch.randn((basis.ndim, nvec), dtype=torch.float64, device="cuda", generator=g) + \
+        1j * torch.randn((basis.ndim, nvec), dtype=torch.float64, device="cuda", generator=g)
+    v = (v / torch.linalg.vector_norm(v, dim=0, keepdim=True)).contiguous()
+    want, outs = _both(L, basis, v, nv, nvec)
+    for call, got in enumerate(outs):
+        assert np.all(np.isfinite(got))
+        assert np.abs(got - want).max() <= 1e-12 * max(1.0, np.abs(want).max()), f"call {call}"
+        assert np.allclose(np.trace(got, axis1=1, axis2=2).real, nelec, atol=1e-10)
 
 
 def test_denmat_static_rejects_oversize(cuda):

@@ -45,7 +45,6 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-packed", action="store_true", help="no packed forms of H_n, H_f (CSR products only)")
-    ap.add_argument("--tiles", action="store_true", help="also offer the tiled layout of H_f to the autotuner")
     ap.add_argument("--ed", action="store_true",
                     help="plain FP64 ED instead of RIXS: lowest eigenpairs of a 10 + 14 orbital model")
     ap.add_argument("--ed-nbath", type=int, default=14)
@@ -124,7 +123,7 @@ def kernel_case_all(args):
     summary): Fock unranking (the 2.7 M-state C(24,12) sector too), the count/fill builds of
     H_f, H_n, D_in and D_out, the one-column SpMV and the 6-column SpMM, two Lanczos steps
     on H_n (6 columns, with shifts and projections) and H_f (256 columns) on the CSR, packed
-    and tiled forms with their builders, two MINRES steps on H_n, the continued fraction
+    forms with the packer, two MINRES steps on H_n, the continued fraction
     (768 pole sets x 2000 points), the density matrix, the packed SpMM (narrow and wide
     forms), the Gram-Schmidt and CholeskyQR passes of the eigensolver, the few-column Lanczos
     products with one row per lane group, and 16 Lanczos steps with streamed projections."""
@@ -158,8 +157,6 @@ def kernel_case_all(args):
     device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1, packed=Pf))
     device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=4, threads=1024, blocks_per_sm=2, packed=Pf))
     device.krylov(Hf, W, 2, apply=dict(col_group=32, tiles=2, threads=256, blocks_per_sm=4, packed=Pf))
-    L = device.tiles_for(Hf, bi)
-    device.krylov(Hf, W, 2, apply=dict(layout=L))
     device.minres(Hn, x1, 1e-300, 2, alpha=-1.0, sigma=40 + 0.6j)
     K, nk = 768, 150
     al = 20 * torch.rand((K, nk), dtype=torch.float64, device="cuda", generator=g)
@@ -192,15 +189,27 @@ def kernel_case_all(args):
                       "nnz_Dout": Dout.nnz}))
 
 
-# DRAM bytes (read + write) of one H_f Lanczos product over 256 of the 768 columns, from the
-# `--kernel-case all` ncu capture (profiles/all_kernels_dram.md), per launch shape
-# (packed, columns per group, tiles, threads, blocks per SM, chunked)
-HF_DRAM_256 = {
-    (False, 32, 2, 1024, 1, 0): 5.835e9,
-    (True, 32, 2, 1024, 1, 0): 5.111e9,
-    (True, 32, 4, 1024, 2, 0): 7.834e9,
-    (True, 32, 2, 256, 4, 0): 5.136e9,
-}
+def shape_key(kernel, cfg, k, rows):
+    """Canonical name of one apply launch (kernel, launch shape, columns, rows): the key under
+    which an ncu summary in profiles/ records that launch's DRAM bytes."""
+    cfg = cfg or {}
+    keys = ("col_group", "tiles", "threads", "blocks_per_sm", "chunked", "rowslot")
+    shape = " ".join(f"{x}={int(cfg.get(x, 0) or 0)}" for x in keys)
+    return f"{kernel} {shape} k={int(k)} rows={int(rows)}"
+
+
+def measured_traffic(key):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) for the launch
+    named `key`, from a line `dram_bytes_per_launch: <bytes> | <key>` in one of the ncu
+    summaries under profiles/; None when no capture of exactly that launch exists."""
+    import glob
+    for f in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        for ln in open(f):
+            if ln.startswith("dram_bytes_per_launch:") and "|" in ln:
+                val, k = ln.split(":", 1)[1].split("|", 1)
+                if k.strip() == key:
+                    return float(val), os.path.basename(f)
+    return None
 
 
 def load_peaks():
@@ -250,8 +259,6 @@ def setup_gpu(args, ngs=3):
     edge = float(e_n[0] - gs_e[0])
     P = rixs.RixsProblem(Hn=Hn, Hf=Hf, Din=Din, Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v.contiguous())
     P.packed.update(packed)
-    if args.tiles and not args.c64:
-        P.tiles["hf"] = device.tiles_for(Hf, bi)
     omegas = edge - 2.0 + np.linspace(0.0, 10.0, args.n_omega)
     eloss = np.linspace(-0.5, 12.0, args.n_eloss)
     torch.cuda.synchronize()
@@ -397,10 +404,12 @@ def _cf_np(alpha, beta, norm, neff, z):
     return norm / (z - a[0] - g)
 
 
-def accuracy_report(P, res, plain, omegas, eloss, w_idx, nkryl, npin=2, npout=2, ngs=3):
+def accuracy_report(P, res, plain, omegas, eloss, w_idx, nkryl, start, npin=2, npout=2, ngs=3):
     """Batched vs the plain FP64 one-RHS path at one incident energy, next to the conditioning
     floor of the reference's final-state Lanczos (150 steps, no reorthogonalisation): the
-    change of the plain path's own spectrum when its start vector moves by 1e-14 relative."""
+    change of the plain path's own spectrum when its start vector moves by 1e-14 relative.
+    start: the batched path's final-state start vectors of that incident energy, column
+    (po * npin + pi) * ngs + g."""
     import torch
     from edrixs_b200 import device, rixs
     n_om = len(omegas)
@@ -449,34 +458,52 @@ def accuracy_report(P, res, plain, omegas, eloss, w_idx, nkryl, npin=2, npout=2,
                 floor = max(floor, float(np.abs(sq - sp).max() / scale))
         out["spectra_rel_err"][f"gamma_f_{gamma}"] = err
         out["conditioning_floor"][f"gamma_f_{gamma}"] = floor
-    # both against the exact resolvent -Im <phi|(z - H_f)^-1|phi>, converged MINRES per point:
-    # the 150-step continued fraction's own error, which bounds what "equal to the reference"
-    # can mean pointwise
+    # the exact resolvent -Im <phi|(z - H_f)^-1|phi>, MINRES converged to 1e-13 per point, of
+    # both paths' final-state start vectors: the plain phi_p = D_out^+ x_p (one-RHS MINRES,
+    # src/linsys.f90) and the batched phi_b = D_out^+ x_b (shared Krylov spaces).  Their
+    # difference is what batching changes; the 150-step continued fraction's own error
+    # (vs_exact_resolvent) is the reference algorithm's and the same for both.
     npts = 12
     pts = np.linspace(0.0, 8.0, npts)
-    for gamma in (1.0, 0.1):
-        eb = ep = 0.0
+    gammas = (1.0, 0.1)
+    sv_err = 0.0
+    ex = {}  # (pi, po, g) -> {gamma: (exact of phi_p, exact of phi_b)}
+    for pi in range(npin):
+        for po in range(npout):
+            for g in range(ngs):
+                b = device.spmm(P.Din[pi], P.gs_v[:, g].contiguous())
+                z = complex(omegas[w_idx] + P.gs_e[g], 0.6)
+                x, _, _ = device.minres(P.Hn, b, 1e-10, 1000, alpha=-1.0, sigma=z)
+                phi_p = device.spmm(P.Dout[po], x)
+                phi_b = start[:, (po * npin + pi) * ngs + g].contiguous()
+                nphi = float(torch.linalg.vector_norm(phi_p))
+                sv_err = max(sv_err, float(torch.linalg.vector_norm(phi_b - phi_p)) / nphi)
+                for gamma in gammas:
+                    zz = pts + P.gs_e[g] + 1j * gamma
+                    sp_, sb_ = np.zeros(npts), np.zeros(npts)
+                    for q, zq in enumerate(zz):
+                        for phi, dst in ((phi_p, sp_), (phi_b, sb_)):
+                            xe, _, _ = device.minres(P.Hf, phi, 1e-13 * nphi, 60000, alpha=-1.0, sigma=complex(zq))
+                            dst[q] = -float(torch.vdot(phi, xe).imag)
+                    ex.setdefault((pi, po, g), {})[gamma] = (sp_, sb_, zz)
+    out["start_vector_rel_err"] = sv_err
+    for gamma in gammas:
+        eb = ep = eres = 0.0
         for pi in range(npin):
             for po in range(npout):
-                se = np.zeros(npts)
-                sb = np.zeros(npts)
-                sp = np.zeros(npts)
+                se_p, se_b, sb, sp = (np.zeros(npts) for _ in range(4))
                 for g in range(ngs):
-                    b = device.spmm(P.Din[pi], P.gs_v[:, g].contiguous())
-                    z = complex(omegas[w_idx] + P.gs_e[g], 0.6)
-                    x, _, _ = device.minres(P.Hn, b, 1e-10, 1000, alpha=-1.0, sigma=z)
-                    phi = device.spmm(P.Dout[po], x)
-                    zz = pts + P.gs_e[g] + 1j * gamma
-                    nphi = float(torch.linalg.vector_norm(phi))
-                    for q, zq in enumerate(zz):
-                        xe, _, _ = device.minres(P.Hf, phi, 1e-13 * nphi, 60000, alpha=-1.0, sigma=complex(zq))
-                        se[q] += w[g] * -float(torch.vdot(phi, xe).imag)
+                    e_p, e_b, zz = ex[(pi, po, g)][gamma]
+                    se_p += w[g] * e_p
+                    se_b += w[g] * e_b
                     sb += w[g] * -_cf_np(*batched_set(pi, po, g), zz).imag
                     sp += w[g] * -_cf_np(*plain_set(pi, po, g), zz).imag
-                scale = np.abs(se).max()
-                eb = max(eb, float(np.abs(sb - se).max() / scale))
-                ep = max(ep, float(np.abs(sp - se).max() / scale))
+                scale = np.abs(se_p).max()
+                eb = max(eb, float(np.abs(sb - se_p).max() / scale))
+                ep = max(ep, float(np.abs(sp - se_p).max() / scale))
+                eres = max(eres, float(np.abs(se_b - se_p).max() / scale))
         out.setdefault("vs_exact_resolvent", {"points": npts})[f"gamma_f_{gamma}"] = dict(batched=eb, plain=ep)
+        out.setdefault("batched_vs_plain_resolvent", {"points": npts, "tol": 1e-6})[f"gamma_f_{gamma}"] = eres
     # the first Lanczos coefficients, before orthogonality is lost, are well conditioned
     d = 0.0
     for key in plain:
@@ -567,20 +594,24 @@ def run_ours(args):
 
     r_hf = roof(st["hf_nnz"], st["hf_rows"], st["k_hf"], st["hf_apply_ms"], st["hf_iterations"], args.c64,
                 P.packed.get("hf") if st.get("hf_packed") else None)
-    # DRAM bytes per launch from one ncu capture of the same kernel and launch shape on 256 of
-    # the 768 columns (the kernel case above), scaled by the number of 64-column sweeps
-    cfg = tuned.get("hf_k768") or {}
-    shape = (bool(st.get("hf_packed")), cfg.get("col_group"), cfg.get("tiles"), cfg.get("threads"),
-             cfg.get("blocks_per_sm"), cfg.get("chunked"))
-    if not st.get("hf_tiled") and not args.c64 and st["k_hf"] == 768 and shape in HF_DRAM_256:
-        r_hf["traffic"] = 3 * HF_DRAM_256[shape]
-        r_hf["traffic_source"] = "ncu dram__bytes_read+write on 256 columns (same shape) x 3"
     r_hn = roof(st["hn_nnz"], st["hn_rows"], st["k_hn"], st["hn_apply_ms"], st["hn_iterations"], args.c64,
                 P.packed.get("hn") if st.get("hn_packed") else None)
     dom, sec = (r_hf, r_hn) if r_hf["total_ms"] >= r_hn["total_ms"] else (r_hn, r_hf)
-    hf_kernel = ("k_lanczos_apply_tiles" if st.get("hf_tiled") else
-                 "k_lanczos_apply_packed" if st.get("hf_packed") else "k_lanczos_apply")
-    hn_kernel = "k_lanczos_apply_packed" if st.get("hn_packed") else "k_lanczos_apply"
+
+    def kname(packed, cfg):
+        rs = bool(cfg and cfg.get("rowslot"))
+        return ("k_lanczos_apply_packed" if packed else "k_lanczos_apply") + ("_rs" if rs else "")
+
+    hf_kernel = kname(st.get("hf_packed"), tuned.get(f"hf_k{st['k_hf']}"))
+    hn_kernel = kname(st.get("hn_packed"), tuned.get(f"hn_k{st['k_hn']}"))
+    # DRAM traffic of the launch shape that ran, from an ncu capture of exactly that launch
+    for r, kern, cfg_key, k_, rows_ in ((r_hf, hf_kernel, f"hf_k{st['k_hf']}", st["k_hf"], st["hf_rows"]),
+                                        (r_hn, hn_kernel, f"hn_k{st['k_hn']}", st["k_hn"], st["hn_rows"])):
+        key = shape_key(kern, tuned.get(cfg_key), k_, rows_)
+        r["launch"] = key
+        got = measured_traffic(key)
+        if got is not None:
+            r["traffic"], r["traffic_source"] = int(got[0]), f"ncu dram__bytes_read.sum + write.sum ({got[1]})"
     dom_name = f"{hf_kernel} on H_f (768 columns)" if dom is r_hf else f"{hn_kernel} on H_n (6 columns)"
 
     extra = {"spmv_roofline": spmv_roofline(P, peak)}
@@ -601,7 +632,12 @@ def run_ours(args):
         extra["plain_fp64_one_rhs"] = {"seconds_per_omega_in": round(plain_s, 3),
                                        "value": round(1.0 / plain_s, 4), "unit": UNIT,
                                        "batched_over_plain": round(value / ws / (1.0 / plain_s), 2)}
-        extra["accuracy"] = accuracy_report(P, res, plain, omegas, eloss, w_idx, args.nkryl)
+        # the batched start vectors of this incident energy (the same deterministic solve as
+        # the timed steps, run once more to keep them)
+        cols = [((po * 2 + pi) * 3 + g) * n_om + w_idx for po in range(2) for pi in range(2) for g in range(3)]
+        rs = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, start_cols=cols, **kw)
+        extra["accuracy"] = accuracy_report(P, rs, plain, omegas, eloss, w_idx, args.nkryl, rs.start)
+        del rs
         extra["rel_err_vs_fp64_plain"] = extra["accuracy"]["spectra_rel_err"]["gamma_f_0.1"]
 
     cpu = None
@@ -619,13 +655,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64" if args.c64 else "c128",
             "data": "synthetic (seeded SIAM inputs; reference atomic tensors)",
-            "config": {"workload": f"batched RIXS L-edge: 6 core + {m.nv} valence spin-orbitals, N_v={args.nelec}, "
-                                   f"dim_n={P.Hn.nrows}, dim_f={P.Hf.nrows}, {n_om} omega_in x 2 pol_in x 2 pol_out "
-                                   f"x 3 gs, Gamma_c=0.6, MINRES tol 1e-10, {args.nkryl}-step final Lanczos, "
-                                   f"{len(eloss)} loss points",
-                       "nnz_Hn": P.Hn.nnz, "nnz_Hf": P.Hf.nnz, "parallelism": f"replicas x{ws}",
-                       "autotuned_apply": tuned,
-                       "l2": "inputs larger than L2 (H_n CSR > 1 GB) between timed steps"},
+            "config": workload_config(args, P.Hn.nrows, P.Hf.nrows, P.Hn.nnz, P.Hf.nnz, ws),
+            "autotuned_apply": tuned,
             "latency_ms": {"p50": round(float(np.percentile(lat_ms, 50)), 2),
                            "p99": round(float(np.percentile(lat_ms, 99)), 2)},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -976,36 +1007,102 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def workload_config(args, dim_n, dim_f, nnz_n, nnz_f, ws):
+    """The config block both arms print (the same workload, so the arms compare)."""
+    nv = 10 + args.nbath
+    return {"workload": f"batched RIXS L-edge: 6 core + {nv} valence spin-orbitals, N_v={args.nelec}, "
+                        f"dim_n={dim_n}, dim_f={dim_f}, {args.n_omega} omega_in x 2 pol_in x 2 pol_out "
+                        f"x 3 gs, Gamma_c=0.6, MINRES tol 1e-10, {args.nkryl}-step final Lanczos, "
+                        f"{args.n_eloss} loss points",
+            "nnz_Hn": int(nnz_n), "nnz_Hf": int(nnz_f), "parallelism": f"replicas x{ws}",
+            "l2": "inputs larger than L2 (H_n CSR > 1 GB) between timed steps"}
+
+
 def run_reference(args):
+    """The reference's algorithm on the host cores, measured: each step is ONE full
+    (omega_in, pol_in, pol_out, gs) point of the workload, as src/rixs_driver.f90 runs it --
+    MINRES (src/linsys.f90:3-128) on (omega + E_g + i Gamma_c) - H_n to the absolute
+    tolerance 1e-10, D_out^+ x, the 150-step Lanczos (src/lanczos.f90:210-303) on H_f, and
+    the continued fraction on the 2000-point loss grid -- in the oracle's C/OpenMP FP64
+    restatement on every host thread.  The timed steps walk the incident-energy window and
+    the 12 (pol_in, pol_out, gs) combinations, so their mean is the mean point of the
+    workload.  Not timed: the per-point H_n / H_f rebuilds the Fortran performs
+    (src/rixs_driver.f90:130-133,199); the shifted matrix is H_n with omega + E_g + i Gamma_c
+    written onto its diagonal, which favours the CPU.  value = omega_in points per second =
+    1 / (12 x mean seconds per point); ms_per_step = mean measured milliseconds per point."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import scipy.sparse.linalg as sla
     from oracle import pyoracle as orc
     m, t = workload_terms(args.nbath, args.nelec)
     nv, N = m.nv, args.nelec
-    fi = orc.fock_full_N(nv, N)
+    fi, fn = orc.fock_full_N(nv, N), orc.fock_full_N(nv, N + 1)
     Hf = orc.build_csr("ham_i", fi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
     gs_e, gs_v = orc.ed_eigs(Hf, 3, dense_below=0, tol=1e-10)
-    omega = 5.0  # middle of the incident-energy window; the MINRES count is fixed below
-    its = 300    # representative MINRES iteration count at Gamma_c = 0.6, tol 1e-10
-    samples = []
-    desc = ""
-    for i in range(args.warmup + args.steps):
-        per_point, desc, secs = cpu_sample(args, t, (gs_e, gs_v), omega, its, minres_its=30, krylov_steps=30)
-        if i >= args.warmup:
-            samples.append(per_point)
-    per_point = float(np.mean(samples))
+    # -H_n with an explicit diagonal (ham_sign = -1, omega = 0: src/ham.f90:156-176)
+    A0 = orc.build_csr("ham_n", fn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6, ham_sign=-1.0,
+                       omega=0j)
+    rows = np.repeat(np.arange(A0.nrows, dtype=np.int64), np.diff(A0.row_ptr))
+    dpos = np.nonzero(A0.col == rows)[0]
+    del rows
+    assert len(dpos) == A0.nrows
+    Din = [orc.build_csr("trans_i", fn, d, fock_right=fi, num_val_orbs=nv, num_core_orbs=6) for d in t["din"]]
+    Dout = [orc.build_csr("trans_f", fi, d, fock_right=fn, num_val_orbs=nv, num_core_orbs=6) for d in t["dout"]]
+    # the absorption edge as the GPU arm places it: lowest eigenvalue of H_n minus E_0
+    op = sla.LinearOperator((A0.nrows, A0.nrows), matvec=lambda x: -orc.matvec(A0, x), dtype=np.complex128)
+    e_n = sla.eigsh(op, k=1, which="SA", tol=1e-6, ncv=24)[0]
+    edge = float(np.min(e_n) - gs_e[0])
+    omegas = edge - 2.0 + np.linspace(0.0, 10.0, args.n_omega)
+    eloss = np.linspace(-0.5, 12.0, args.n_eloss)
+    A = orc.CSR(A0.row_ptr, A0.col, A0.val.copy(), A0.ncols)
+    seeds = {}
+
+    def point(w_idx, pi, po, g):
+        key = (pi, g)
+        if key not in seeds:
+            seeds[key] = orc.matvec(Din[pi], gs_v[:, g])
+        z = complex(omegas[w_idx] + gs_e[g], 0.6)
+        A.val[dpos] = A0.val[dpos] + z
+        x, its, _ = orc.minres(A, seeds[key], 1e-10, 1000)
+        phi = orc.matvec(Dout[po], x)
+        al, be, nrm, neff = orc.build_krylov(Hf, phi, args.nkryl)
+        zz = eloss + gs_e[g] + 0.1j
+        gz = np.zeros_like(zz)
+        for i in range(neff - 1, 0, -1):
+            gz = be[i - 1] ** 2 / (zz - al[i] - gz)
+        spec = -(nrm / (zz - al[0] - gz)).imag / np.pi
+        return its, spec
+
+    combos = [(pi, po, g) for pi in range(2) for po in range(2) for g in range(3)]
+    w_steps = np.linspace(0, args.n_omega - 1, max(args.steps, 1)).round().astype(int)
+    for i in range(args.warmup):
+        point(args.n_omega // 2, *combos[i % 12])
+    secs, its = [], []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        it, _ = point(int(w_steps[i]), *combos[i % 12])
+        secs.append(time.perf_counter() - t0)
+        its.append(it)
+    per_point = float(np.mean(secs))
     value = 1.0 / (12 * per_point)
-    line = {"metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(12 * per_point * 1e3, 3), "higher_is_better": True,
+    desc = (f"oracle (C/OpenMP FP64 restatement of linsys.f90 + lanczos.f90), {orc.num_threads()} threads: "
+            f"{args.steps} full (omega_in, pol_in, pol_out, gs) points measured, incident energies spread over "
+            f"the window, MINRES to 1e-10 (mean {np.mean(its):.0f} iterations) on dim {A0.nrows} + "
+            f"{args.nkryl}-step Lanczos on dim {Hf.nrows} + continued fraction on {len(eloss)} points; "
+            f"per-point H_n/H_f rebuilds of rixs_driver.f90 not timed; 12 points per omega_in")
+    line = {"metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(per_point * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "impl": "reference",
             "data": "synthetic (seeded SIAM inputs; reference atomic tensors)",
-            "config": {"workload": f"batched RIXS L-edge: 6 core + {nv} valence spin-orbitals, N_v={N}, "
-                                   f"one omega_in (12 pol-pair x gs points) per step"},
-            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
+            # every row of this H_n has a diagonal entry, so the shifted matrix has H_n's nonzeros
+            "config": workload_config(args, A0.nrows, Hf.nrows, A0.nnz, Hf.nnz, ws),
+            "step": "one (omega_in, pol_in, pol_out, gs) point",
+            "minres_iterations": {"mean": float(np.mean(its)), "max": int(np.max(its))},
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
                              "sample": desc},
-            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 

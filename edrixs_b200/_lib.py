@@ -42,12 +42,6 @@ class Csr(ctypes.Structure):
                 ("val_type", ctypes.c_int)]
 
 
-class Tiles(ctypes.Structure):
-    _fields_ = [("nrows", i64), ("ntile_r", i32), ("ntile_c", i32), ("tile_r", vp), ("tile_c", vp),
-                ("npiece", i64), ("nent", i64), ("nhdr", i64), ("piece_ptr", vp), ("piece_ctile", vp),
-                ("piece_rows", vp), ("piece_ent", vp), ("piece_hdr", vp), ("hdr", vp), ("lcol", vp), ("val", vp)]
-
-
 class Packed(ctypes.Structure):
     _fields_ = [("nrows", i64), ("nnz", i64), ("row_ptr", vp), ("ent", vp), ("vbits", ctypes.c_int),
                 ("nval", ctypes.c_int), ("vals", vp), ("diag", vp), ("vidx", vp)]
@@ -61,7 +55,7 @@ class KrylovOpts(ctypes.Structure):
                 ("apply_col_group", ctypes.c_int), ("apply_threads", ctypes.c_int),
                 ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int),
                 ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int),
-                ("apply_layout", ctypes.POINTER(Tiles)), ("apply_packed", ctypes.POINTER(Packed)),
+                ("apply_packed", ctypes.POINTER(Packed)),
                 ("proj_window", ctypes.c_int), ("nacc", ctypes.c_int), ("acc_col", vp), ("acc_coef", vp),
                 ("acc_out", ctypes.POINTER(vp)), ("acc_ld", i64), ("v0_ld", i64),
                 ("apply_rowslot", ctypes.c_int)]
@@ -86,10 +80,6 @@ _SIGS = {
                                       ctypes.c_size_t, vp]),
     "edx_spmm": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.c_int, ctypes.c_int, vp, i64, vp, i64, dbl, dbl,
                                 dbl, dbl, dbl, dbl, ctypes.c_int, vp]),
-    "edx_tiles_workspace": (ctypes.c_int, [ctypes.POINTER(Csr), i32, i32, ctypes.POINTER(ctypes.c_size_t)]),
-    "edx_tiles_count": (ctypes.c_int, [ctypes.POINTER(Csr), i32, vp, i32, vp, ctypes.POINTER(i64),
-                                       ctypes.POINTER(i64), ctypes.POINTER(i64), vp, ctypes.c_size_t, vp]),
-    "edx_tiles_fill": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(Tiles), vp, ctypes.c_size_t, vp]),
     "edx_pack_workspace": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(ctypes.c_size_t)]),
     "edx_pack_count": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.c_int, ctypes.POINTER(i64),
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), vp, ctypes.c_size_t,

@@ -381,205 +381,6 @@ __global__ void __launch_bounds__(NT) k_lanczos_apply_rs(int64_t n, const int64_
     }
 }
 
-// ---- K9a on the tiled layout ------------------------------------------------------------
-// One block per (row tile, 32 columns).  The block walks the pieces of its row tile; for
-// each piece it stages the column tile of V_cur (32 columns, up to EDX_TILE_COLS_MAX rows)
-// and the piece's entries in shared memory with cp.async, double-buffered so that the next
-// piece loads while this one computes.  Consecutive pieces of one column tile share the
-// staged tile.  Warp w owns local rows w, w + 32, ...; lane = column, so an entry is a
-// shared-memory broadcast and its x row one 512-byte shared-memory read.  Every row sums
-// its entries in ascending column order.
-constexpr int TL_NT = 1024;
-constexpr int TL_NW = TL_NT / 32;
-constexpr int TL_RPW = EDX_TILE_ROWS_MAX / TL_NW;  // rows per warp
-constexpr int TL_HDR = EDX_TILE_ROWS_MAX + 8;       // header slots staged per piece
-constexpr size_t TL_X_BYTES = (size_t)EDX_TILE_COLS_MAX * 32 * sizeof(double2);
-constexpr size_t TL_VAL_BYTES = (size_t)EDX_TILE_PIECE_MAX * sizeof(double2);
-constexpr size_t TL_STAGE_BYTES = TL_VAL_BYTES + EDX_TILE_PIECE_MAX + TL_HDR * sizeof(uint16_t);
-constexpr size_t TL_SMEM = 2 * TL_X_BYTES + 2 * TL_STAGE_BYTES;
-static_assert(TL_RPW * TL_NW == EDX_TILE_ROWS_MAX, "row tile must split evenly over the warps");
-static_assert(EDX_TILE_PIECE_MAX % 16 == 0 && TL_HDR % 8 == 0, "16-byte staging chunks");
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
-}
-// No L2 cache-policy operand here: this kernel with cp.async.cg ... .L2::cache_hint (policy from
-// createpolicy evict_first) raised "illegal instruction" on B200, and the same kernel with
-// plain cp.async and bounds/alignment self-checks ran clean on the same input.
-__device__ __forceinline__ void cp_async16_full(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-struct TilesView {
-    const int32_t* tile_r;
-    const int32_t* tile_c;
-    const int32_t* piece_ptr;
-    const int32_t* piece_ctile;
-    const int32_t* piece_rows;
-    const int64_t* piece_ent;
-    const int64_t* piece_hdr;
-    const uint16_t* hdr;
-    const uint8_t* lcol;
-    const double2* val;
-};
-
-__device__ __forceinline__ void tl_stage(const TilesView& T, int p, bool load_x, double2* xs, double2* ev,
-                                         uint8_t* el, uint16_t* eh, const double2* __restrict__ Vc, int k,
-                                         int col0) {
-    const int tid = threadIdx.x;
-    if (load_x) {
-        const int C = __ldg(T.piece_ctile + p);
-        const int32_t cs = __ldg(T.tile_c + C);
-        const int rc = __ldg(T.tile_c + C + 1) - cs;
-        for (int i = tid; i < rc * 32; i += TL_NT) {
-            const int row = i >> 5, c = i & 31;
-            const int gc = col0 + c;
-            const bool ok = gc < k;
-            cp_async16(xs + i, Vc + (int64_t)(cs + row) * k + (ok ? gc : col0), ok ? 16 : 0);
-        }
-    }
-    const int64_t e0 = __ldg(T.piece_ent + p);
-    const int ne = (int)(__ldg(T.piece_ent + p + 1) - e0);
-    for (int i = tid; i < ne; i += TL_NT) cp_async16_full(ev + i, T.val + e0 + i);
-    for (int i = tid; i < (ne >> 4); i += TL_NT) cp_async16_full(el + 16 * i, T.lcol + e0 + 16 * i);
-    const int rows = __ldg(T.piece_rows + p);
-    const int nh = (rows >> 16) - (rows & 0xffff) + 1;
-    const int64_t h0 = __ldg(T.piece_hdr + p);
-    for (int i = tid; i < ((nh + 7) >> 3); i += TL_NT) cp_async16_full(eh + 8 * i, T.hdr + h0 + 8 * i);
-}
-
-__global__ void __launch_bounds__(TL_NT, 1)
-    k_lanczos_apply_tiles(TilesView T, const double2* __restrict__ Vc, double2* __restrict__ Vp, KrylovState S,
-                          unsigned* __restrict__ gticket, int it) {
-    extern __shared__ __align__(16) unsigned char tl_smem[];
-    // buffers addressed arithmetically (an indexed array of pointers would live in local memory)
-    auto xs = [&](int b) { return reinterpret_cast<double2*>(tl_smem + b * TL_X_BYTES); };
-    auto stg = [&](int b) { return tl_smem + 2 * TL_X_BYTES + b * TL_STAGE_BYTES; };
-    auto ev = [&](int b) { return reinterpret_cast<double2*>(stg(b)); };
-    auto el = [&](int b) { return reinterpret_cast<uint8_t*>(stg(b) + TL_VAL_BYTES); };
-    auto eh = [&](int b) { return reinterpret_cast<uint16_t*>(stg(b) + TL_VAL_BYTES + EDX_TILE_PIECE_MAX); };
-    __shared__ double sh[TL_NW * 32];
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int k = S.k;
-    const int R = blockIdx.x;
-    const int col0 = blockIdx.y * 32;
-    const int32_t r0 = __ldg(T.tile_r + R);
-    const int nr = __ldg(T.tile_r + R + 1) - r0;
-    const int p_beg = __ldg(T.piece_ptr + R), p_end = __ldg(T.piece_ptr + R + 1);
-    double2 acc[TL_RPW];
-#pragma unroll
-    for (int t = 0; t < TL_RPW; ++t) acc[t] = make_double2(0.0, 0.0);
-
-    int xcur = 0;
-    if (p_beg < p_end) {
-        tl_stage(T, p_beg, true, xs(0), ev(0), el(0), eh(0), Vc, k, col0);
-        cp_async_commit();
-    }
-    for (int p = p_beg; p < p_end; ++p) {
-        const int s = (p - p_beg) & 1;
-        const int cp_ = __ldg(T.piece_ctile + p);
-        int xnext = xcur;
-        if (p + 1 < p_end) {
-            const bool newx = __ldg(T.piece_ctile + p + 1) != cp_;
-            xnext = newx ? (xcur ^ 1) : xcur;
-            tl_stage(T, p + 1, newx, xs(xnext), ev(s ^ 1), el(s ^ 1), eh(s ^ 1), Vc, k, col0);
-            cp_async_commit();
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
-        const int rows = __ldg(T.piece_rows + p);
-        const int ra = rows & 0xffff, rb = rows >> 16;
-        const double2* X = xs(xcur);
-        const double2* E = ev(s);
-        const uint8_t* L = el(s);
-        const uint16_t* H = eh(s);
-#pragma unroll
-        for (int t = 0; t < TL_RPW; ++t) {
-            const int lr = warp + t * TL_NW;
-            if (lr >= ra && lr < rb) {
-                const int a = H[lr - ra], b = H[lr - ra + 1];
-                double2 sacc = acc[t];
-                int e = a;
-                for (; e + 1 < b; e += 2) {
-                    const int l0 = L[e], l1 = L[e + 1];
-                    const double2 v0 = E[e], v1 = E[e + 1];
-                    const double2 x0 = X[l0 * 32 + lane], x1 = X[l1 * 32 + lane];
-                    sacc = fma_c(v0, x0, sacc);
-                    sacc = fma_c(v1, x1, sacc);
-                }
-                if (e < b) sacc = fma_c(E[e], X[L[e] * 32 + lane], sacc);
-                acc[t] = sacc;
-            }
-        }
-        __syncthreads();
-        xcur = xnext;
-    }
-
-    // W = A V_cur - beta_{i-1} V_prev into V_prev; alpha partial Re(conj(v) w) per column
-    const int gc = col0 + lane;
-    const bool ok = gc < k;
-    const double bprev = (ok && it > 0) ? S.beta[gc] * S.sprev[gc] : 0.0;
-    const double scur = ok ? S.scur[gc] : 0.0;
-    double apart = 0.0;
-#pragma unroll
-    for (int t = 0; t < TL_RPW; ++t) {
-        const int lr = warp + t * TL_NW;
-        if (lr < nr && ok) {
-            const int64_t o = (int64_t)(r0 + lr) * k + gc;
-            const double2 vp = Vp[o];
-            double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
-            w.x = w.x + scur * acc[t].x;
-            w.y = w.y + scur * acc[t].y;
-            Vp[o] = w;
-            const double2 vc = Vc[o];
-            apart += vc.x * w.x + vc.y * w.y;
-        }
-    }
-    sh[warp * 32 + lane] = apart;
-    __syncthreads();
-    if (warp == 0) {
-        double s = 0.0;
-        for (int w = 0; w < TL_NW; ++w) s += sh[w * 32 + lane];
-        if (ok) S.part[(int64_t)R * k + gc] = s;
-    }
-    // the last block of this column group adds the row tiles' partials in row-tile order
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = (atomicAdd(gticket + blockIdx.y, 1u) == gridDim.x - 1u);
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    {
-        const int q = warp;  // row tiles q, q + 32, ... summed by warp q
-        double s = 0.0;
-        if (ok)
-            for (int b = q; b < (int)gridDim.x; b += TL_NW) s += __ldcg(S.part + (int64_t)b * k + gc);
-        sh[q * 32 + lane] = s;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        double a = 0.0;
-        for (int w = 0; w < TL_NW; ++w) a += sh[w * 32 + lane];
-        if (ok) {
-            a *= scur;
-            S.alpha[gc] = a;
-            if (S.active[gc]) S.alpha_out[(int64_t)gc * S.maxn + it] = a;
-        }
-        if (lane == 0) gticket[blockIdx.y] = 0u;
-    }
-}
-
 // ---- K9b: W -= alpha v_i, beta = |W|, next scales -----------------------------------------
 // v_i = scur * U_i, so W -= (alpha * scur) U_i.  The last block of each column group (one
 // ticket per group) finishes its columns: beta from the per-block partials (the group's
@@ -991,26 +792,6 @@ static int apply_packed(const edx_packed* P, const double2* Vc, double2* Vp, con
     return fail(EDX_ERR_INVALID, "krylov: bad column group %d", cfg.kw);
 }
 
-static int apply_tiles(const edx_tiles* L, const double2* Vc, double2* Vp, const KrylovState& S, unsigned* gt,
-                       int it, cudaStream_t st) {
-    static bool smem_set[EDX_MAX_DEVICES] = {};
-    int dev = 0;
-    EDX_CUDA(cudaGetDevice(&dev));
-    EDX_REQUIRE(dev >= 0 && dev < EDX_MAX_DEVICES, "edx_krylov: device ordinal %d out of range", dev);
-    if (!smem_set[dev]) {
-        EDX_CUDA(cudaFuncSetAttribute(k_lanczos_apply_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)TL_SMEM));
-        smem_set[dev] = true;
-    }
-    TilesView T{L->tile_r,    L->tile_c,    L->piece_ptr, L->piece_ctile,
-                L->piece_rows, L->piece_ent, L->piece_hdr, L->hdr,
-                L->lcol,       reinterpret_cast<const double2*>(L->val)};
-    dim3 grid((unsigned)L->ntile_r, (unsigned)((S.k + 31) / 32));
-    k_lanczos_apply_tiles<<<grid, TL_NT, TL_SMEM, st>>>(T, Vc, Vp, S, gt, it);
-    EDX_CHECK_LAUNCH();
-    return EDX_OK;
-}
-
 #define EDX_KW_SWITCH(kw, KERNEL, GRID, ...)                                                  \
     switch (kw) {                                                                              \
     case 1: KERNEL<1><<<GRID, KT, 0, st>>>(__VA_ARGS__); break;                               \
@@ -1026,7 +807,7 @@ struct KrylovWs {
     double *alpha, *beta, *part, *scur, *sprev;
     int *active, *n_active, *n_open;
     unsigned* ticket;
-    unsigned* gticket;  // one per 32 columns (tiled product)
+    unsigned* gticket;  // one per 32 columns (per-group finish of the orthogonalisation)
     ShiftState* sst;
     double2* wbuf;
 };
@@ -1090,7 +871,6 @@ extern "C" int edx_krylov_workspace(int64_t n, int k, const edx_krylov_opts* opt
     EDX_REQUIRE(bytes != nullptr && n >= 1 && k >= 1 && maxn >= 1, "edx_krylov_workspace: bad arguments");
     SizeOnly s;
     int gx = num_sms() * 8;  // largest grid any kernel here uses
-    if (opts && opts->apply_layout) gx = std::max(gx, (int)opts->apply_layout->ntile_r);
     krylov_layout(s, n, k, opts ? opts->nshift : 0, maxn, gx, nullptr);
     *bytes = s.s.bytes();
     return EDX_OK;
@@ -1142,15 +922,6 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     EDX_REQUIRE(cfg.threads == 256 || cfg.threads == 1024, "edx_krylov: apply_threads must be 256 or 1024");
     EDX_REQUIRE(bps >= 1 && bps * cfg.threads <= 8 * 256, "edx_krylov: apply_blocks_per_sm out of range");
     cfg.gx = num_sms() * bps;
-    const edx_tiles* layout = opts ? opts->apply_layout : nullptr;
-    if (layout) {
-        EDX_REQUIRE(A->val_type == EDX_C128, "edx_krylov: the tiled product needs a complex128 matrix");
-        EDX_REQUIRE(layout->nrows == n && layout->ntile_r >= 1 && layout->npiece >= 1 && layout->tile_r &&
-                        layout->tile_c && layout->piece_ptr && layout->piece_ctile && layout->piece_rows &&
-                        layout->piece_ent && layout->piece_hdr && layout->hdr && layout->lcol && layout->val,
-                    "edx_krylov: apply_layout does not describe this matrix");
-        EDX_REQUIRE((k + 31) / 32 <= 65535, "edx_krylov: too many columns for the tiled product");
-    }
     const edx_packed* packed = opts ? opts->apply_packed : nullptr;
     if (packed) {
         EDX_REQUIRE(packed->nrows == n && packed->row_ptr && packed->diag &&
@@ -1160,12 +931,10 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
                     "edx_krylov: apply_packed does not describe this matrix");
     }
     if (cfg.rowslot)
-        EDX_REQUIRE(!layout && cfg.kw <= 16 && k <= cfg.kw,
-                    "edx_krylov: apply_rowslot needs k <= apply_col_group <= 16 (and no tiled layout)");
+        EDX_REQUIRE(cfg.kw <= 16 && k <= cfg.kw, "edx_krylov: apply_rowslot needs k <= apply_col_group <= 16");
     const int kw = pow2_kw(k);  // layout of the element-wise recurrence kernels
     const int gy = (k + kw - 1) / kw;
     int gx = num_sms() * 8;
-    if (layout) gx = std::max(gx, (int)layout->ntile_r);
     Workspace w(d_work, work_bytes);
     KrylovWs ws;
     krylov_layout(w, n, k, nshift, maxn, gx, &ws);
@@ -1268,9 +1037,7 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
             evs.push_back(e1);
             EDX_CUDA(cudaEventRecord(e0, st));
         }
-        if (layout)
-            rc = apply_tiles(layout, Vc, Vp, S, ws.gticket, it, st);
-        else if (packed)
+        if (packed)
             rc = apply_packed(packed, Vc, Vp, S, it, cfg, st);
         else
             rc = (A->val_type == EDX_C128) ? apply_v<double2>(A, Vc, Vp, S, it, cfg, st)

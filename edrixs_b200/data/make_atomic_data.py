@@ -77,6 +77,7 @@ def main(ref_path, out_path):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python edrixs_b200/data/make_atomic_data.py /path/to/edrixs-reference")
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "atomic_dp.npz")
-    main(ref, out)
+    main(sys.argv[1], out)

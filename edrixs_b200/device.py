@@ -12,7 +12,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import BuildDesc, Csr, KrylovOpts, Packed, Tiles, call
+from ._lib import BuildDesc, Csr, KrylovOpts, Packed, call
 
 C128, C64 = _lib.EDX_C128, _lib.EDX_C64
 HAM_I, HAM_N, TRANS_I, TRANS_F = _lib.EDX_HAM_I, _lib.EDX_HAM_N, _lib.EDX_TRANS_I, _lib.EDX_TRANS_F
@@ -194,94 +194,6 @@ def build_csr(mode, left: Basis, hopping, coulomb=None, right: Optional[Basis] =
 
 
 # ------------------------------------------------------------------------------------
-# tiled layout (edx_tiles_*)
-# ------------------------------------------------------------------------------------
-
-TILE_ROWS_MAX, TILE_COLS_MAX, TILE_PIECE_MAX = 256, 128, 1024
-
-
-def fock_tiles(states: torch.Tensor, max_len):
-    """Cut an ascending list of distinct states into runs that share their high bits: the
-    largest shift p whose runs of equal (state >> p) hold at most max_len states (p = 0 gives
-    runs of one state, so a shift always exists).  Returns the int32 tile starts [ntile+1]
-    on the states' device."""
-    s = states.to(torch.int64)
-    n = s.numel()
-    zero = torch.zeros(1, dtype=torch.int64, device=s.device)
-    end = torch.full((1,), n, dtype=torch.int64, device=s.device)
-    for p in range(63, -1, -1):
-        key = torch.bitwise_right_shift(s, p)
-        bounds = torch.cat([zero, torch.nonzero(torch.diff(key) != 0).flatten() + 1, end])
-        if int(torch.diff(bounds).max()) <= max_len:
-            return bounds.to(torch.int32)
-    raise ValueError("fock_tiles: states must be distinct and ascending")
-
-
-@dataclass
-class TiledLayout:
-    """Device arrays of an edx_tiles layout (see include/edx.h); keeps them alive."""
-    nrows: int
-    tile_r: torch.Tensor
-    tile_c: torch.Tensor
-    piece_ptr: torch.Tensor
-    piece_ctile: torch.Tensor
-    piece_rows: torch.Tensor
-    piece_ent: torch.Tensor
-    piece_hdr: torch.Tensor
-    hdr: torch.Tensor
-    lcol: torch.Tensor
-    val: torch.Tensor
-
-    @property
-    def npiece(self):
-        return self.piece_ctile.numel()
-
-    def desc(self):
-        return Tiles(self.nrows, self.tile_r.numel() - 1, self.tile_c.numel() - 1, _ptr(self.tile_r),
-                     _ptr(self.tile_c), self.npiece, self.lcol.numel(), self.hdr.numel(), _ptr(self.piece_ptr),
-                     _ptr(self.piece_ctile), _ptr(self.piece_rows), _ptr(self.piece_ent), _ptr(self.piece_hdr),
-                     _ptr(self.hdr), _ptr(self.lcol), _ptr(self.val))
-
-    def nbytes(self):
-        return sum(t.numel() * t.element_size() for t in (self.tile_r, self.tile_c, self.piece_ptr,
-                                                           self.piece_ctile, self.piece_rows, self.piece_ent,
-                                                           self.piece_hdr, self.hdr, self.lcol, self.val))
-
-
-def build_tiles(A: CSR, tile_r, tile_c):
-    """Tiled layout of the square complex128 matrix A for the given row / column tile starts."""
-    require_cuda()
-    tile_r = tile_r.to(device="cuda", dtype=torch.int32).contiguous()
-    tile_c = tile_c.to(device="cuda", dtype=torch.int32).contiguous()
-    ntr, ntc = tile_r.numel() - 1, tile_c.numel() - 1
-    d = A.desc()
-    ws = ctypes.c_size_t(0)
-    call("edx_tiles_workspace", ctypes.byref(d), ntr, ntc, ctypes.byref(ws))
-    w = _work(ws.value)
-    npiece, nent, nhdr = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
-    st = _stream()
-    call("edx_tiles_count", ctypes.byref(d), ntr, _ptr(tile_r), ntc, _ptr(tile_c), ctypes.byref(npiece),
-         ctypes.byref(nent), ctypes.byref(nhdr), _ptr(w), ws.value, st)
-    i32, i64 = dict(dtype=torch.int32, device="cuda"), dict(dtype=torch.int64, device="cuda")
-    L = TiledLayout(A.nrows, tile_r, tile_c, torch.empty(ntr + 1, **i32), torch.empty(npiece.value, **i32),
-                    torch.empty(npiece.value, **i32), torch.empty(npiece.value + 1, **i64),
-                    torch.empty(npiece.value, **i64), torch.empty(nhdr.value, dtype=torch.int16, device="cuda"),
-                    torch.empty(nent.value, dtype=torch.uint8, device="cuda"),
-                    torch.empty(nent.value, dtype=torch.complex128, device="cuda"))
-    t = L.desc()
-    call("edx_tiles_fill", ctypes.byref(d), ctypes.byref(t), _ptr(w), ws.value, st)
-    return L
-
-
-def tiles_for(A: CSR, basis: Basis):
-    """Tiled layout of a Hamiltonian over `basis` (rows and columns in basis order): row
-    tiles of <= 256 states and column tiles of <= 128 states that share their high bits."""
-    if basis.ndim != A.nrows or A.nrows != A.ncols:
-        raise ValueError("tiles_for: the basis must index the rows and columns of A")
-    return build_tiles(A, fock_tiles(basis.states, TILE_ROWS_MAX), fock_tiles(basis.states, TILE_COLS_MAX))
-
-
-# ------------------------------------------------------------------------------------
 # packed form (edx_pack_*)
 # ------------------------------------------------------------------------------------
 
@@ -425,8 +337,6 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
     only the last B projected vectors."""
     if isinstance(A, PackedMatrix):
         apply = dict(apply or {}, packed=A)
-        if apply.get("layout") is not None:
-            raise ValueError("krylov: a packed matrix has no tiled layout")
     kcols = V0.reshape(V0.shape[0], -1).shape[1]
     if apply and apply.get("packed") is not None and "rowslot" not in apply and kcols <= 16 \
             and "col_group" not in apply:
@@ -504,10 +414,6 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
         opts.apply_tiles = int(apply.get("tiles", 0))
         opts.apply_prefetch = int(apply.get("prefetch", 0))
         opts.apply_rowslot = int(apply.get("rowslot", 0))
-        if apply.get("layout") is not None:
-            tdesc = apply["layout"].desc()
-            opts.apply_layout = ctypes.pointer(tdesc)
-            keep += [tdesc]
         if apply.get("packed") is not None:
             pdesc = apply["packed"].desc()
             opts.apply_packed = ctypes.pointer(pdesc)
@@ -596,6 +502,8 @@ def cf_spectrum(neff, alpha, beta, e0, norm, weight, omega, gamma, per_set=False
     dev = alpha.device
     f64 = dict(dtype=torch.float64, device=dev)
     omega = torch.as_tensor(omega, **f64).contiguous()
+    if not torch.is_tensor(gamma):  # a numpy broadcast view is read-only: copy it first
+        gamma = np.array(gamma, dtype=np.float64)
     gamma = torch.broadcast_to(torch.as_tensor(gamma, **f64), omega.shape).contiguous()
     out = torch.zeros((nset, omega.numel()) if per_set else (omega.numel(),), **f64)
     # every argument tensor is bound to a name: a temporary freed before the launch could

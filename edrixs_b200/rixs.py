@@ -51,26 +51,20 @@ class RixsProblem:
     gs_e: np.ndarray
     gs_v: torch.Tensor                       # (n_i, ngs) complex128
     meta: dict = field(default_factory=dict)
-    tiles: dict = field(default_factory=dict)   # "hf" / "hn" -> device.TiledLayout of that matrix
     packed: dict = field(default_factory=dict)  # "hf" / "hn" -> device.PackedMatrix of that matrix
 
     def nbytes(self):
         b = self.Hn.nbytes() + self.Hf.nbytes() + sum(D.nbytes() for D in self.Din + self.Dout)
         if self.Hn.val64 is not None:
             b += self.Hn.nnz * 8
-        b += sum(L.nbytes() for L in self.tiles.values())
         b += sum(M.nbytes() for M in self.packed.values())
         return b + self.gs_v.numel() * 16
 
 
-def _apply_args(cfg, layout, packed, c64):
+def _apply_args(cfg, packed, c64):
     """Launch arguments of one Krylov call: the autotuner's choice, else the packed product
     when a packed form exists, else libedx's defaults."""
     if cfg is not None:
-        if cfg.get("tiled"):
-            if layout is None:
-                raise ValueError("the tuned launch shape needs the tiled layout")
-            return dict(layout=layout)
         if cfg.get("packed"):
             if packed is None:
                 raise ValueError("the tuned launch shape needs the packed form")
@@ -91,6 +85,8 @@ class RixsResult:
     stats: dict = field(default_factory=dict)  # kernel launch counts and timings
     spectra_gs: Optional[np.ndarray] = None  # per ground state, before the Boltzmann sum:
     #                                          (n_omega, n_eloss, n_pol_in * n_pol_out, ngs)
+    start: Optional[torch.Tensor] = None     # (n_f, len(start_cols)) final-state start vectors
+    #                                          D_out^+ x of the requested columns
 
 
 def _stream_needed(P, k, maxn):
@@ -103,14 +99,17 @@ def _stream_needed(P, k, maxn):
 
 def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, linsys_tol=1e-10,
                  linsys_max=1000, temperature=300.0, c64=False, final_block=None, timing=False, autotune=False,
-                 stream=None, stream_window=8, seeds=None, c64_final=None, per_gs=False):
+                 stream=None, stream_window=8, seeds=None, c64_final=None, per_gs=False, start_cols=None):
     """RIXS spectra of every (omega_in, pol_in, pol_out, gs) of one request.
     stream: None (automatic), True or False -- whether D_out^+ v_i is folded into the
     final-state start vectors as the Lanczos vectors appear (two passes over H_n) instead of
     being stored for every v_i.  seeds: the block D_in(pol_in)|g> (n_n, npin * ngs), column
     p_in * ngs + g, when the caller computed it already (P.Din is then not used).  c64: the
     H_n products (MINRES part) in complex64; c64_final: the H_f products too (default: as c64).
-    per_gs: also return the spectra of each ground state before the Boltzmann sum."""
+    per_gs: also return the spectra of each ground state before the Boltzmann sum.
+    start_cols: final-state columns (p_out, p_in, g, omega order: column
+    ((p_out * n_pol_in + p_in) * ngs + g) * n_omega + w) whose start vectors D_out^+ x to
+    return in ``start``."""
     c64_f = c64 if c64_final is None else bool(c64_final)
     omegas = np.asarray(omegas, dtype=np.float64)
     eloss = np.asarray(eloss, dtype=np.float64)
@@ -121,12 +120,10 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     K_hf = npout * k_hn * n_om if final_block is None else int(final_block)
     if autotune:
         from . import tune
-        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64, layout=P.tiles.get("hn"),
-                                                             packed=P.packed.get("hn"))
-        P.meta[("apply", "hf", K_hf, c64_f)] = tune.tune_apply(P.Hf, K_hf, c64=c64_f, layout=P.tiles.get("hf"),
-                                                               packed=P.packed.get("hf"))
-    cfg_hn = _apply_args(P.meta.get(("apply", "hn", k_hn, c64)), P.tiles.get("hn"), P.packed.get("hn"), c64)
-    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64_f)), P.tiles.get("hf"), P.packed.get("hf"), c64_f)
+        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64, packed=P.packed.get("hn"))
+        P.meta[("apply", "hf", K_hf, c64_f)] = tune.tune_apply(P.Hf, K_hf, c64=c64_f, packed=P.packed.get("hf"))
+    cfg_hn = _apply_args(P.meta.get(("apply", "hn", k_hn, c64)), P.packed.get("hn"), c64)
+    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64_f)), P.packed.get("hf"), c64_f)
     gam_c = np.broadcast_to(np.asarray(gamma_c, dtype=np.float64), (n_om,))
     dev = P.gs_v.device
     # 1. seeds (n_n, npin*ngs), column c = p_in*ngs + g
@@ -186,6 +183,7 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
         stats["launches"] += 4 + npout + r2.apply_launches * (2 + 2 * npout) + \
             npout * ((m + int(stream_window) - 1) // int(stream_window))
         del r2, Y
+    start = V0[:, list(start_cols)].clone() if start_cols is not None else None
     # 4. final-state Lanczos, all pole sets as one block (optionally in chunks of columns)
     blk = K if final_block is None else int(final_block)
     A = torch.zeros((K, nkryl), dtype=torch.float64, device=dev)
@@ -201,7 +199,7 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
         hf_it += rf.apply_launches
         stats["launches"] += 2 + 2 * rf.apply_launches  # norm, start; apply + orth per step
     stats.update(hf_apply_ms=hf_ms if timing else None, hf_iterations=hf_it, hf_nnz=P.Hf.nnz, hf_rows=P.Hf.nrows,
-                 k_hf=blk, hf_tiled=bool(cfg_hf and cfg_hf.get("layout") is not None),
+                 k_hf=blk,
                  hf_packed=bool(cfg_hf and cfg_hf.get("packed") is not None),
                  hn_packed=bool(cfg_hn and cfg_hn.get("packed") is not None))
     del V0
@@ -215,7 +213,7 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     stats["launches"] += 1
     per_g = spec.permute(3, 4, 1, 0, 2).reshape(n_om, ne, npin * npout, ngs).cpu().numpy() if per_gs else None
     return RixsResult(out.cpu().numpy(), dict(alpha=A, beta=B, norm=NRM, neff=NEFF, e0=e0), iters, resid, steps,
-                      stats, per_g)
+                      stats, per_g, start)
 
 
 def rixs_request(P: RixsProblem, gs_v_host, omegas, gamma_c, eloss, gamma_f, **kw):

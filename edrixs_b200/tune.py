@@ -36,11 +36,10 @@ def candidates(k):
     return out
 
 
-def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None, packed=None):
-    """Fastest launch shape for k columns on A.  With a tiled layout or a packed form of A
-    (complex128 only) those products are timed too; the result then carries "tiled": 1 or
-    "packed": 1."""
-    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64), layout is not None, packed is not None)
+def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, packed=None):
+    """Fastest launch shape for k columns on A.  With a packed form of A (complex128 only)
+    its products are timed too; the result then carries "packed": 1."""
+    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64), packed is not None)
     if key in _cache:
         return _cache[key]
     dev = A.row_ptr.device
@@ -57,12 +56,7 @@ def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, layout=None,
         cands = cands + [dict(c, packed=1, rowslot=0) for c in candidates(k)]
         if k <= 16:  # one row per lane group
             cands += [dict(c, packed=1, rowslot=1) for c in candidates(k) if c["chunked"] == 0]
-    if layout is not None and not c64:
-        cands = [dict(tiled=1)] + cands
-
     def args_of(cfg):
-        if cfg.get("tiled"):
-            return dict(layout=layout)
         if cfg.get("packed"):
             return dict(cfg, packed=packed)
         return cfg

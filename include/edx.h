@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define EDX_ABI_VERSION 3
+#define EDX_ABI_VERSION 4
 
 /* status codes */
 #define EDX_OK 0
@@ -130,56 +130,6 @@ typedef struct edx_csr {
 int edx_spmm(const edx_csr* A, int k, int vec_type, const void* d_x, int64_t ldx, void* d_y,
              int64_t ldy, double alpha_re, double alpha_im, double sigma_re, double sigma_im,
              double beta_re, double beta_im, int col_group, void* stream);
-
-/* ---------------------------------------------------------------------------------- */
-/* Tiled layout of a square matrix (no counterpart in the reference, whose matvec_csr     */
-/* src/spmv.f90:73-103 walks the CSR directly)                                         */
-/* ---------------------------------------------------------------------------------- */
-
-/* Rows and columns are cut into tiles of consecutive indices (row tiles of at most
- * EDX_TILE_ROWS_MAX rows, column tiles of at most EDX_TILE_COLS_MAX columns).  For a
- * Hamiltonian in a Fock basis, a tile is a run of states that share their high orbitals
- * (the bath occupation of an impurity model), so the entries of a row tile fall into few
- * column tiles.  The entries of each (row tile, column tile) pair are stored together,
- * cut at row boundaries into pieces of at most EDX_TILE_PIECE_MAX entries, so that a
- * block can stage one column tile of a multi-vector in shared memory and use it for every
- * row of its row tile.  Within a row the entries keep the CSR's ascending column order.
- *
- * Piece p covers local rows ra..rb-1 of its row tile (piece_rows[p] = ra | rb << 16) and
- * column tile piece_ctile[p]; its entries start at piece_ent[p] (a multiple of 16) and
- * row ra + i owns entries piece_ent[p] + hdr[piece_hdr[p] + i] .. + hdr[piece_hdr[p] + i + 1]
- * - 1 (piece_hdr[p] is a multiple of 8).  lcol is the column minus the column tile's first
- * column.  Pieces of row tile t are piece_ptr[t] .. piece_ptr[t+1]-1, ordered by column
- * tile, then by row. */
-#define EDX_TILE_ROWS_MAX 256
-#define EDX_TILE_COLS_MAX 128
-#define EDX_TILE_PIECE_MAX 1024
-typedef struct edx_tiles {
-    int64_t nrows;
-    int32_t ntile_r, ntile_c;
-    const int32_t* tile_r;     /* device int32[ntile_r+1], tile_r[0] = 0, tile_r[ntile_r] = nrows */
-    const int32_t* tile_c;     /* device int32[ntile_c+1], same for the columns */
-    int64_t npiece, nent, nhdr;
-    const int32_t* piece_ptr;  /* device int32[ntile_r+1] */
-    const int32_t* piece_ctile;/* device int32[npiece] */
-    const int32_t* piece_rows; /* device int32[npiece] */
-    const int64_t* piece_ent;  /* device int64[npiece+1], piece_ent[npiece] = nent */
-    const int64_t* piece_hdr;  /* device int64[npiece] */
-    const uint16_t* hdr;       /* device uint16[nhdr] */
-    const uint8_t* lcol;       /* device uint8[nent] */
-    const void* val;           /* device complex128[nent] */
-} edx_tiles;
-
-/* Scratch bytes of edx_tiles_count / edx_tiles_fill for matrix A. */
-int edx_tiles_workspace(const edx_csr* A, int32_t ntile_r, int32_t ntile_c, size_t* bytes);
-/* Pass 1: sizes of the layout of complex128 A (square, nnz < 2^31) under the given tiles
- * (device arrays, checked here).  Synchronises `stream`. */
-int edx_tiles_count(const edx_csr* A, int32_t ntile_r, const int32_t* d_tile_r, int32_t ntile_c,
-                    const int32_t* d_tile_c, int64_t* npiece, int64_t* nent, int64_t* nhdr,
-                    void* d_work, size_t work_bytes, void* stream);
-/* Pass 2: T->tile_*, ntile_*, npiece, nent, nhdr as returned by pass 1 and every output
- * array allocated by the caller; d_work must still hold what pass 1 left in it. */
-int edx_tiles_fill(const edx_csr* A, edx_tiles* T, void* d_work, size_t work_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Packed form of a square matrix (no counterpart in the reference)                    */
@@ -296,14 +246,9 @@ typedef struct edx_krylov_opts {
     int apply_chunked;
     int apply_tiles;
     int apply_prefetch;
-    /* tiled layout of the same matrix (edx_tiles_fill), or NULL.  With a layout the product
-     * runs one block per (row tile, 32 columns): each column tile of the current Lanczos
-     * vectors is staged in shared memory once and used for all rows of the row tile.
-     * complex128 matrices only; the launch-shape fields above are then ignored. */
-    const edx_tiles* apply_layout;
     /* packed form of the same matrix (edx_pack_fill), or NULL.  With it the product reads
      * one 32-bit word per off-diagonal entry and the value from a table in shared memory,
-     * with the launch-shape fields above (the tiled layout takes precedence). */
+     * with the launch-shape fields above. */
     const edx_packed* apply_packed;
     /* streaming projections, for problems where P_p V (every projected Lanczos vector) does
      * not fit in memory.  With proj_window = B > 0, proj_out[p] holds only the last B

@@ -47,6 +47,13 @@ class Packed(ctypes.Structure):
                 ("nval", ctypes.c_int), ("vals", vp), ("diag", vp), ("vidx", vp)]
 
 
+class Kron(ctypes.Structure):
+    _fields_ = [("nrows", i64), ("nslab", i32), ("nb", i32), ("nah", i32), ("n_alo", i32), ("max_rows", i32),
+                ("slab_off", vp), ("slab_m", vp), ("slab_cfg", vp), ("hyb_a", vp), ("t_cre", vp), ("t_ann", vp),
+                ("src_ptr", vp), ("src_slab", vp), ("src_kind", vp), ("src_coef", vp), ("b_off", vp), ("b_cfg", vp),
+                ("b_nbr", vp), ("b_diag", vp)]
+
+
 class KrylovOpts(ctypes.Structure):
     _fields_ = [("nproj", ctypes.c_int), ("proj", ctypes.POINTER(Csr)), ("proj_out", ctypes.POINTER(vp)),
                 ("nshift", ctypes.c_int), ("shift_col", vp), ("shift_z", vp), ("shift_tol", dbl),
@@ -55,7 +62,7 @@ class KrylovOpts(ctypes.Structure):
                 ("apply_col_group", ctypes.c_int), ("apply_threads", ctypes.c_int),
                 ("apply_blocks_per_sm", ctypes.c_int), ("apply_chunked", ctypes.c_int),
                 ("apply_tiles", ctypes.c_int), ("apply_prefetch", ctypes.c_int),
-                ("apply_packed", ctypes.POINTER(Packed)),
+                ("apply_packed", ctypes.POINTER(Packed)), ("apply_kron", ctypes.POINTER(Kron)),
                 ("proj_window", ctypes.c_int), ("nacc", ctypes.c_int), ("acc_col", vp), ("acc_coef", vp),
                 ("acc_out", ctypes.POINTER(vp)), ("acc_ld", i64), ("v0_ld", i64),
                 ("apply_rowslot", ctypes.c_int)]
@@ -87,6 +94,10 @@ _SIGS = {
     "edx_pack_fill": (ctypes.c_int, [ctypes.POINTER(Csr), ctypes.POINTER(Packed), vp, ctypes.c_size_t, vp]),
     "edx_spmm_packed": (ctypes.c_int, [ctypes.POINTER(Packed), ctypes.c_int, vp, i64, vp, i64, dbl, dbl, dbl, dbl,
                                        dbl, dbl, ctypes.c_int, vp]),
+    "edx_kron_spmm_workspace": (ctypes.c_int, [ctypes.POINTER(ctypes.c_size_t)]),
+    "edx_kron_spmm": (ctypes.c_int, [ctypes.POINTER(Kron), ctypes.c_int, vp, vp, ctypes.c_int, vp, ctypes.c_size_t,
+                                     vp]),
+    "edx_permute_rows": (ctypes.c_int, [i64, ctypes.c_int, vp, i64, vp, vp, i64, vp]),
     "edx_gs_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "edx_gs_dot": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp, ctypes.c_size_t, vp]),
     "edx_gs_update": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp]),

@@ -1,0 +1,530 @@
+// edx_kron.cu -- the slab (impurity x bath) product: k_lanczos_apply_kron (fused Lanczos step
+// and plain Y = H X), edx_kron_spmm, edx_permute_rows.
+//
+// In the slab order every row of slab s (impurity/core configuration I, m bath electrons)
+// takes its inputs from a short list of whole source slabs (edx_kron.src_*): the slabs of
+// H_A's row s, and the slabs I + a / I - a one bath electron away.  A block owns a run of
+// slabs for CW columns; one thread stages each source slab into a ring of shared-memory
+// buffers with 2-D tiled tensor loads (cp.async.bulk.tensor, 32-row boxes, completion on an
+// mbarrier; no multicast), and every thread accumulates its rows x one column from shared
+// memory: a scaled copy for H_A sources, and for hybridisation sources one bath-electron hop
+// per occupied (or empty) bath orbital, whose target row is a table lookup.  So the only
+// global traffic is the source slabs (from L2, contiguous rows), the block's own output rows
+// and a few KB of tables; no matrix entries are streamed.
+//
+// Every wait on a staged load is bounded (KR_WAIT_LIMIT rounds of mbarrier.try_wait): a load
+// that never arrives sets the error flag, the block waits (again bounded) for the loads it
+// still has in flight and returns, and the host reports EDX_ERR_CUDA.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "edx_krylov.cuh"
+#include "edx_spmm.cuh"
+
+namespace edx {
+
+constexpr int KR_NT = 256;       // threads per block
+constexpr int KR_BOXR = 32;      // rows per tensor-load box
+constexpr int KR_NBUF = 3;       // source slabs staged ahead
+constexpr uint32_t KR_WAIT_LIMIT = 1u << 21;
+
+struct KronView {
+    const int32_t* slab_off;
+    const int32_t* slab_m;
+    const uint32_t* slab_cfg;
+    const int32_t* hyb_a;
+    const double2* t_cre;
+    const double2* t_ann;
+    const int64_t* src_ptr;
+    const int32_t* src_slab;
+    const int32_t* src_kind;
+    const double2* src_coef;
+    const int32_t* b_off;
+    const uint16_t* b_cfg;
+    const uint16_t* b_nbr;
+    const double2* b_diag;
+    int nslab, nb, nah, n_alo;
+};
+
+static KronView view_of(const edx_kron* K) {
+    return KronView{K->slab_off,
+                    K->slab_m,
+                    K->slab_cfg,
+                    K->hyb_a,
+                    reinterpret_cast<const double2*>(K->t_cre),
+                    reinterpret_cast<const double2*>(K->t_ann),
+                    K->src_ptr,
+                    K->src_slab,
+                    K->src_kind,
+                    reinterpret_cast<const double2*>(K->src_coef),
+                    K->b_off,
+                    K->b_cfg,
+                    K->b_nbr,
+                    reinterpret_cast<const double2*>(K->b_diag),
+                    K->nslab,
+                    K->nb,
+                    K->nah,
+                    K->n_alo};
+}
+
+// ---- mbarrier and tensor-load primitives (PTX ISA: mbarrier, cp.async.bulk.tensor) --------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// true once the phase with this parity has completed; false after KR_WAIT_LIMIT rounds
+__device__ __noinline__ bool mbar_wait_bounded(uint64_t* b, unsigned parity) {
+    for (uint32_t i = 0; i < KR_WAIT_LIMIT; ++i) {
+        if (mbar_try_wait(b, parity)) return true;
+        if (i >= 8) __nanosleep(128);
+    }
+    return false;
+}
+// 2-D tiled tensor load of one box into shared memory; completion counted on `bar`.  The
+// innermost coordinate x is a multiple of 2 doubles (16 bytes) by construction.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// parity of the A-side sign (src/fock.f90:38-68) of c+_a c_b (cre) and c+_b c_a (ann) on a
+// row of a slab with compressed A configuration cfg and m bath electrons; a = compressed
+// index of the A orbital, n_alo = A orbitals below the bath (edrixs_b200/kron.py)
+__device__ __forceinline__ int sig_cre(uint32_t cfg, int m, int a, int n_alo) {
+    const uint32_t lo = (1u << n_alo) - 1u;
+    return (__popc(cfg & lo) + __popc(cfg & ((1u << a) - 1u)) + (a >= n_alo ? m - 1 : 0)) & 1;
+}
+__device__ __forceinline__ int sig_ann(uint32_t cfg, int m, int a, int n_alo) {
+    const uint32_t lo = (1u << n_alo) - 1u;
+    return (__popc(cfg & ((1u << a) - 1u)) + (a >= n_alo ? m : 0) + __popc(cfg & lo) - (a < n_alo ? 1 : 0)) & 1;
+}
+
+// ---- the slab product ---------------------------------------------------------------------
+// grid (gx, column tiles); block b owns slabs b, b + gx, ...; thread (g, c) owns rows
+// g, g + G, ... (RPT of them) of each slab in column c0 + c.  LANCZOS: the fused step of
+// k_lanczos_apply_packed (W = scur (H U_i) - beta_{i-1} sprev U_{i-1} into Y = V_prev, alpha
+// partials, the last block of each column tile finishes alpha in block order); otherwise
+// Y = H X.
+template <int CW, int RPT, bool LANCZOS>
+__global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const __grid_constant__ CUtensorMap tm,
+                                                              const double2* __restrict__ X, double2* __restrict__ Y,
+                                                              KrylovState S, int k, int it, int stage_rows,
+                                                              unsigned* __restrict__ tile_ticket,
+                                                              int* __restrict__ err) {
+    constexpr int G = KR_NT / CW;
+    extern __shared__ __align__(128) unsigned char kr_smem[];
+    // tensor-load destinations must start on a 128-byte boundary: align the ring explicitly
+    // (the host asks for 128 spare bytes)
+    double2* stages = reinterpret_cast<double2*>(kr_smem + ((128u - (smem_addr(kr_smem) & 127u)) & 127u));
+    const int stage_elems = stage_rows * CW;
+    double2* tcre = stages + KR_NBUF * stage_elems;
+    double2* tann = tcre + K.nah * K.nb;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tann + K.nah * K.nb);
+    __shared__ double red[KR_NT];
+    __shared__ bool sh_last;
+
+    const int tid = threadIdx.x;
+    const int g = tid / CW, c = tid % CW;
+    const bool act = g < G;
+    const int c0 = blockIdx.y * CW;
+    const int gcol = c0 + c;
+    const bool colok = act && gcol < k;
+
+    for (int i = tid; i < K.nah * K.nb; i += KR_NT) {
+        tcre[i] = K.t_cre[i];
+        tann[i] = K.t_ann[i];
+    }
+    if (tid == 0) {
+        for (int b = 0; b < KR_NBUF; ++b) mbar_init(&bar[b], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // producer cursor (thread 0): the next source to stage is source p_beg + p_j of slab
+    // p_slab (every slab has at least its own slab as a source)
+    int p_slab = blockIdx.x, p_j = 0;
+    int64_t p_beg = 0, p_end = 0;
+    if (p_slab < K.nslab) {
+        p_beg = K.src_ptr[p_slab];
+        p_end = K.src_ptr[p_slab + 1];
+    }
+    unsigned issued = 0;
+    auto issue_next = [&]() -> bool {
+        while (p_slab < K.nslab && p_beg + p_j >= p_end) {
+            p_slab += gridDim.x;
+            p_j = 0;
+            if (p_slab < K.nslab) {
+                p_beg = K.src_ptr[p_slab];
+                p_end = K.src_ptr[p_slab + 1];
+            }
+        }
+        if (p_slab >= K.nslab) return false;
+        const int sl = K.src_slab[p_beg + p_j];
+        ++p_j;
+        const int r0 = K.slab_off[sl];
+        const int rows = K.slab_off[sl + 1] - r0;
+        const int nbox = (rows + KR_BOXR - 1) / KR_BOXR;
+        const int st = (int)(issued % KR_NBUF);
+        double2* dst = stages + st * stage_elems;
+        mbar_expect_tx(&bar[st], (unsigned)(nbox * KR_BOXR * CW * (int)sizeof(double2)));
+        for (int bx = 0; bx < nbox; ++bx)
+            tma_load_2d(dst + bx * KR_BOXR * CW, &tm, 2 * c0, r0 + bx * KR_BOXR, &bar[st]);
+        ++issued;
+        return true;
+    };
+    if (tid == 0)
+        for (int i = 0; i < KR_NBUF; ++i)
+            if (!issue_next()) break;
+
+    double bprev = 0.0, scur = 0.0;
+    if (LANCZOS && colok) {
+        bprev = it > 0 ? S.beta[gcol] * S.sprev[gcol] : 0.0;
+        scur = S.scur[gcol];
+    }
+    double apart = 0.0;
+    unsigned consumed = 0;
+    bool bad = false;
+    for (int s = blockIdx.x; s < K.nslab && !bad; s += gridDim.x) {
+        const int off = K.slab_off[s];
+        const int R = K.slab_off[s + 1] - off;
+        const int m = K.slab_m[s];
+        const uint32_t cfg = K.slab_cfg[s];
+        const int bo = K.b_off[m];
+        const int64_t sb = K.src_ptr[s], se = K.src_ptr[s + 1];
+        double2 acc[RPT];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) acc[j] = make_double2(0.0, 0.0);
+        for (int64_t js = sb; js < se; ++js) {
+            const int st = (int)(consumed % KR_NBUF);
+            const unsigned par = (consumed / KR_NBUF) & 1u;
+            const bool ok = mbar_wait_bounded(&bar[st], par);
+            if (ok && act) {
+                const double2* Xs = stages + st * stage_elems;
+                const int kind = K.src_kind[js];
+                const int type = kind & 15, q = kind >> 4;
+                if (type <= EDX_KRON_SRC_OWN) {
+                    const double2 v0 = K.src_coef[js];
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        const int r = g + G * j;
+                        if (r < R) {
+                            double2 v = v0;
+                            if (type == EDX_KRON_SRC_OWN) {
+                                const double2 d = __ldg(K.b_diag + bo + r);
+                                v.x += d.x;
+                                v.y += d.y;
+                            }
+                            acc[j] = fma_c(v, Xs[r * CW + c], acc[j]);
+                        }
+                    }
+                } else {
+                    const bool cre = type == EDX_KRON_SRC_CRE;
+                    const int a = K.hyb_a[q];
+                    const int sa = cre ? sig_cre(cfg, m, a, K.n_alo) : sig_ann(cfg, m, a, K.n_alo);
+                    const double2* T = (cre ? tcre : tann) + q * K.nb;
+                    const uint32_t full = (1u << K.nb) - 1u;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        const int r = g + G * j;
+                        if (r < R) {
+                            const uint32_t B = __ldg(K.b_cfg + bo + r);
+                            const uint16_t* nbr = K.b_nbr + (size_t)(bo + r) * K.nb;
+                            uint32_t bits = cre ? B : (~B & full);
+                            while (bits) {
+                                const int b = __ffs(bits) - 1;
+                                bits &= bits - 1u;
+                                const int rs = __ldg(nbr + b);
+                                double2 t = T[b];
+                                if ((sa ^ __popc(B & ((1u << b) - 1u))) & 1) {
+                                    t.x = -t.x;
+                                    t.y = -t.y;
+                                }
+                                acc[j] = fma_c(t, Xs[rs * CW + c], acc[j]);
+                            }
+                        }
+                    }
+                }
+            }
+            ++consumed;
+            // every thread is done with this stage (and all agree whether a load was lost)
+            bad = __syncthreads_or(!ok) != 0;
+            if (bad) break;
+            if (tid == 0) {
+                fence_proxy_async();
+                issue_next();
+            }
+        }
+        if (bad) break;
+        if (colok) {
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+                const int r = g + G * j;
+                if (r < R) {
+                    const int64_t o = (int64_t)(off + r) * k + gcol;
+                    if (LANCZOS) {
+                        const double2 vc = X[o];
+                        const double2 vp = Y[o];
+                        double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
+                        w.x = w.x + scur * acc[j].x;
+                        w.y = w.y + scur * acc[j].y;
+                        Y[o] = w;
+                        apart += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
+                    } else {
+                        Y[o] = acc[j];
+                    }
+                }
+            }
+        }
+    }
+    if (bad) {
+        if (tid == 0) {
+            atomicExch(err, 1);
+            // the loads still in flight land before the block's shared memory is released
+            for (unsigned u = consumed - 1; u < issued; ++u) mbar_wait_bounded(&bar[u % KR_NBUF], (u / KR_NBUF) & 1u);
+        }
+        return;
+    }
+    if (!LANCZOS) return;
+    // alpha partials of this block, then the last block of the column tile adds them in block order
+    red[tid] = colok ? apart : 0.0;
+    __syncthreads();
+    if (tid < CW && c0 + tid < k) {
+        double t = 0.0;
+        for (int gg = 0; gg < G; ++gg) t += red[gg * CW + tid];
+        S.part[(int64_t)blockIdx.x * k + c0 + tid] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) sh_last = atomicAdd(&tile_ticket[blockIdx.y], 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if (!sh_last) return;
+    __threadfence();
+    for (int j = 0; j < CW && c0 + j < k; ++j) {
+        const int col = c0 + j;
+        double t = 0.0;
+        for (int b = tid; b < (int)gridDim.x; b += KR_NT) t += __ldcg(S.part + (int64_t)b * k + col);
+        red[tid] = t;
+        __syncthreads();
+        for (int h = KR_NT / 2; h > 0; h >>= 1) {
+            if (tid < h) red[tid] += red[tid + h];
+            __syncthreads();
+        }
+        if (tid == 0) {
+            const double a = S.scur[col] * red[0];
+            S.alpha[col] = a;
+            if (S.active[col]) S.alpha_out[(int64_t)col * S.maxn + it] = a;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) tile_ticket[blockIdx.y] = 0u;
+}
+
+// ---- host side ----------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+static bool cw_supported(int cw) {
+    return cw == 1 || cw == 2 || cw == 4 || cw == 6 || cw == 8 || cw == 12 || cw == 16;
+}
+
+static int default_cw(int k) {
+    const int ws[] = {1, 2, 4, 6, 8, 12, 16};
+    for (int w : ws)
+        if (w >= k) return w;
+    return 16;
+}
+
+static int stage_rows_of(const edx_kron* K) { return (K->max_rows + KR_BOXR - 1) / KR_BOXR * KR_BOXR; }
+
+static size_t smem_bytes(const edx_kron* K, int cw) {
+    return 128 + (size_t)KR_NBUF * stage_rows_of(K) * cw * sizeof(double2) +
+           2 * (size_t)K->nah * K->nb * sizeof(double2) + KR_NBUF * sizeof(uint64_t);
+}
+
+static int rpt_of(const edx_kron* K, int cw) {
+    const int G = KR_NT / cw;
+    for (int r : {4, 8, 16})
+        if (r * G >= K->max_rows) return r;
+    return 0;
+}
+
+int kron_check(const edx_kron* K) {
+    EDX_REQUIRE(K != nullptr, "slab form: NULL descriptor");
+    EDX_REQUIRE(K->nrows >= 1 && K->nrows < ((int64_t)1 << 31) && K->nslab >= 1 && K->nb >= 1 &&
+                    K->nb <= EDX_KRON_NB_MAX && K->nah >= 0 && K->nah <= EDX_KRON_NAH_MAX && K->n_alo >= 0 &&
+                    K->n_alo <= 31 && K->max_rows >= 1,
+                "slab form: sizes out of range (nrows %lld, nslab %d, nb %d, nah %d)", (long long)K->nrows,
+                K->nslab, K->nb, K->nah);
+    EDX_REQUIRE(K->slab_off && K->slab_m && K->slab_cfg && K->src_ptr && K->src_slab && K->src_kind && K->src_coef &&
+                    K->b_off && K->b_cfg && K->b_nbr && K->b_diag && (K->nah == 0 || (K->hyb_a && K->t_cre && K->t_ann)),
+                "slab form: a device array is missing");
+    return EDX_OK;
+}
+
+int kron_grid_x(const edx_kron* K, int k, int cw) {
+    const size_t sm = smem_bytes(K, cw);
+    int occ = (int)std::min<size_t>(8, (size_t)(227 * 1024) / std::max<size_t>(sm + 2048, 1));
+    if (occ < 1) occ = 1;
+    const int ntile = (k + cw - 1) / cw;
+    const int64_t target = (int64_t)num_sms() * occ * 4;
+    int64_t gx = (target + ntile - 1) / ntile;
+    gx = std::max<int64_t>(1, std::min<int64_t>(gx, K->nslab));
+    return (int)gx;
+}
+
+int kron_tensor_map(const edx_kron* K, const double2* X, int k, int cw, void* out) {
+    auto fn = encode_tiled();
+    if (!fn) return fail(EDX_ERR_CUDA, "slab form: cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t dims[2] = {(cuuint64_t)2 * k, (cuuint64_t)K->nrows};
+    cuuint64_t strides[1] = {(cuuint64_t)2 * k * sizeof(double)};
+    cuuint32_t box[2] = {(cuuint32_t)(2 * cw), (cuuint32_t)KR_BOXR};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double2*>(X),
+                    dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(EDX_ERR_CUDA, "slab form: cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return EDX_OK;
+}
+
+template <int CW, int RPT, bool LANCZOS>
+static int launch_kron_rpt(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
+                           int k, int it, unsigned* tt, int* err, cudaStream_t st) {
+    auto kern = k_lanczos_apply_kron<CW, RPT, LANCZOS>;
+    const size_t sm = smem_bytes(K, CW);
+    EDX_REQUIRE(sm <= 227 * 1024, "slab form: %zu bytes of staged slabs exceed shared memory (use fewer columns)",
+                sm);
+    EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int ntile = (k + CW - 1) / CW;
+    EDX_REQUIRE(ntile <= 65535, "slab form: too many column tiles");
+    dim3 grid(kron_grid_x(K, k, CW), ntile);
+    kern<<<grid, KR_NT, sm, st>>>(view_of(K), *tm, X, Y, S, k, it, stage_rows_of(K), tt, err);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}
+
+template <int CW, bool LANCZOS>
+static int launch_kron_cw(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
+                          int k, int it, unsigned* tt, int* err, cudaStream_t st) {
+    switch (rpt_of(K, CW)) {
+    case 4: return launch_kron_rpt<CW, 4, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 8: return launch_kron_rpt<CW, 8, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 16: return launch_kron_rpt<CW, 16, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    }
+    return fail(EDX_ERR_INVALID, "slab form: slabs of %d rows are too long for %d columns per block", K->max_rows, CW);
+}
+
+template <bool LANCZOS>
+static int launch_kron(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
+                       int k, int it, unsigned* tt, int* err, int cw, cudaStream_t st) {
+    switch (cw) {
+    case 1: return launch_kron_cw<1, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 2: return launch_kron_cw<2, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 4: return launch_kron_cw<4, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 6: return launch_kron_cw<6, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 8: return launch_kron_cw<8, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 12: return launch_kron_cw<12, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 16: return launch_kron_cw<16, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    }
+    return fail(EDX_ERR_INVALID, "slab form: columns per block must be 1, 2, 4, 6, 8, 12 or 16 (got %d)", cw);
+}
+
+int kron_col_group(int k, int requested) { return requested > 0 ? requested : default_cw(k); }
+
+int apply_kron(const edx_kron* K, const void* tmap, const double2* Vc, double2* Vp, const KrylovState& S, int it,
+               unsigned* tile_ticket, int* err, int col_group, cudaStream_t st) {
+    return launch_kron<true>(K, static_cast<const CUtensorMap*>(tmap), Vc, Vp, S, S.k, it, tile_ticket, err,
+                             col_group, st);
+}
+
+__global__ void k_permute_rows(int64_t n, int k, const double2* __restrict__ src, int64_t lds,
+                               const int64_t* __restrict__ idx, double2* __restrict__ dst, int64_t ldd) {
+    const int64_t tot = n * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / k;
+        const int c = (int)(e - i * k);
+        dst[i * ldd + c] = __ldg(src + __ldg(idx + i) * lds + c);
+    }
+}
+
+}  // namespace edx
+
+using namespace edx;
+
+extern "C" int edx_kron_spmm_workspace(size_t* bytes) {
+    EDX_REQUIRE(bytes != nullptr, "edx_kron_spmm_workspace: bad arguments");
+    *bytes = 256;
+    return EDX_OK;
+}
+
+extern "C" int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double* d_y, int col_group, void* d_work,
+                             size_t work_bytes, void* stream) {
+    int rc = kron_check(K);
+    if (rc) return rc;
+    EDX_REQUIRE(k >= 1 && d_x && d_y && d_x != d_y, "edx_kron_spmm: bad arguments");
+    const int cw = kron_col_group(k, col_group);
+    EDX_REQUIRE(cw_supported(cw), "edx_kron_spmm: col_group must be 1, 2, 4, 6, 8, 12 or 16");
+    Workspace w(d_work, work_bytes);
+    int* err = w.take<int>(1);
+    if (!err) return fail(EDX_ERR_WORKSPACE, "edx_kron_spmm: workspace too small");
+    cudaStream_t st = as_stream(stream);
+    EDX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    alignas(64) CUtensorMap tm;
+    if ((rc = kron_tensor_map(K, reinterpret_cast<const double2*>(d_x), k, cw, &tm))) return rc;
+    KrylovState S{};
+    rc = launch_kron<false>(K, &tm, reinterpret_cast<const double2*>(d_x), reinterpret_cast<double2*>(d_y), S, k, 0,
+                            nullptr, err, cw, st);
+    if (rc) return rc;
+    int h = 0;
+    EDX_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EDX_CUDA(cudaStreamSynchronize(st));
+    if (h) return fail(EDX_ERR_CUDA, "edx_kron_spmm: a staged slab load did not arrive within its time limit");
+    return EDX_OK;
+}
+
+extern "C" int edx_permute_rows(int64_t n, int k, const double* d_src, int64_t ld_src, const int64_t* d_idx,
+                                double* d_dst, int64_t ld_dst, void* stream) {
+    EDX_REQUIRE(n >= 0 && k >= 1 && ld_src >= k && ld_dst >= k && (n == 0 || (d_src && d_idx && d_dst)) &&
+                    d_src != d_dst,
+                "edx_permute_rows: bad arguments");
+    if (n == 0) return EDX_OK;
+    cudaStream_t st = as_stream(stream);
+    const int blocks = (int)std::min<int64_t>((n * k + 255) / 256, (int64_t)num_sms() * 16);
+    k_permute_rows<<<blocks, 256, 0, st>>>(n, k, reinterpret_cast<const double2*>(d_src), ld_src, d_idx,
+                                           reinterpret_cast<double2*>(d_dst), ld_dst);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}

@@ -6,10 +6,13 @@
 // polls a "columns still active" counter every few iterations to stop launching.  Reductions
 // are deterministic: every block writes per-column partial sums, and the last block to
 // finish (atomic ticket) adds them in block order.
+#include <cuda.h>
+
 #include <algorithm>
 #include <vector>
 
 #include "edx_fock.cuh"
+#include "edx_krylov.cuh"
 #include "edx_spmm.cuh"
 
 namespace edx {
@@ -21,20 +24,6 @@ int auto_kw(int k);
 int pow2_kw(int k);
 
 constexpr int KT = 256;  // threads per block for the recurrence kernels
-
-// ---- deterministic cross-block reduction --------------------------------------------
-__device__ __forceinline__ bool arrive_last(unsigned* ticket) {
-    __shared__ bool last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned total = gridDim.x * gridDim.y;
-        last = (atomicAdd(ticket, 1u) == total - 1u);
-    }
-    __syncthreads();
-    if (last) __threadfence();
-    return last;
-}
 
 // Sum a per-thread value over threads of the block that share local column c (there are
 // `groups` of them, laid out as sh[g*KW + c]); result written to part[bx*k + gc].
@@ -52,30 +41,6 @@ __device__ __forceinline__ void block_col_partial(double v, bool writer, int g, 
     }
     __syncthreads();
 }
-
-__device__ __forceinline__ double sum_partials(const double* part, int nbx, int k, int gc) {
-    double s = 0.0;
-    for (int b = 0; b < nbx; ++b) s += __ldcg(part + (int64_t)b * k + gc);
-    return s;
-}
-
-struct KrylovState {
-    double* alpha_out;  // [k*maxn]
-    double* beta_out;   // [k*maxn]
-    int32_t* neff;      // [k]
-    double* alpha;      // [k] current alpha
-    double* beta;       // [k] current beta (beta_{i} after K_b; beta_{i-1} during K_a)
-    int* active;        // [k]
-    int* n_active;      // [1]
-    double* part;       // [GX*k]
-    unsigned* ticket;   // [4]
-    // The Lanczos vectors are stored unnormalised: v_i = scur * U_i (U_i = the orthogonalised
-    // residual of the previous step) and v_{i-1} = sprev * U_{i-1}; the products and the
-    // orthogonalisation apply the scales on the fly, so no separate normalisation pass runs.
-    double* scur;       // [k] 1/beta_{i-1} (0 for stopped columns)
-    double* sprev;      // [k] 1/beta_{i-2}
-    int maxn, k;
-};
 
 // ---- K9a: W = A V_cur - beta_{i-1} V_prev (into V_prev), alpha partials ---------------
 // Row mapping: interleaved (warp w of block b takes rows w + NW*(b + B*i)) or chunked (block
@@ -805,8 +770,9 @@ static int apply_packed(const edx_packed* P, const double2* Vc, double2* Vp, con
 struct KrylovWs {
     double2 *Vc, *Vp;
     double *alpha, *beta, *part, *scur, *sprev;
-    int *active, *n_active, *n_open;
+    int *active, *n_active, *n_open, *kron_err;
     unsigned* ticket;
+    unsigned* kticket;  // one per column tile of the slab product
     unsigned* gticket;  // one per 32 columns (per-group finish of the orthogonalisation)
     ShiftState* sst;
     double2* wbuf;
@@ -830,8 +796,9 @@ static void krylov_layout(WS& w, int64_t n, int k, int nshift, int maxn, int gx,
     auto sp = w.template take<double>((size_t)k);
     auto pa = w.template take<double>((size_t)gx * k);
     auto ac = w.template take<int>((size_t)k);
-    auto na = w.template take<int>(2);
+    auto na = w.template take<int>(3);
     auto tk = w.template take<unsigned>(4);
+    auto kt = w.template take<unsigned>((size_t)k);
     auto gt = w.template take<unsigned>((size_t)(k + 31) / 32);
     auto ss = w.template take<ShiftState>((size_t)(nshift > 0 ? nshift : 1));
     auto wb = w.template take<double2>((size_t)(nshift > 0 ? 2 * (size_t)nshift * maxn : 1));
@@ -846,7 +813,9 @@ static void krylov_layout(WS& w, int64_t n, int k, int nshift, int maxn, int gx,
         out->active = ac;
         out->n_active = na;
         out->n_open = na + 1;
+        out->kron_err = na + 2;
         out->ticket = tk;
+        out->kticket = kt;
         out->gticket = gt;
         out->sst = ss;
         out->wbuf = wb;
@@ -871,6 +840,11 @@ extern "C" int edx_krylov_workspace(int64_t n, int k, const edx_krylov_opts* opt
     EDX_REQUIRE(bytes != nullptr && n >= 1 && k >= 1 && maxn >= 1, "edx_krylov_workspace: bad arguments");
     SizeOnly s;
     int gx = num_sms() * 8;  // largest grid any kernel here uses
+    if (opts && opts->apply_kron) {
+        int rc = kron_check(opts->apply_kron);
+        if (rc) return rc;
+        gx = std::max(gx, kron_grid_x(opts->apply_kron, k, kron_col_group(k, opts->apply_col_group)));
+    }
     krylov_layout(s, n, k, opts ? opts->nshift : 0, maxn, gx, nullptr);
     *bytes = s.s.bytes();
     return EDX_OK;
@@ -932,9 +906,19 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     }
     if (cfg.rowslot)
         EDX_REQUIRE(cfg.kw <= 16 && k <= cfg.kw, "edx_krylov: apply_rowslot needs k <= apply_col_group <= 16");
+    const edx_kron* kron = opts ? opts->apply_kron : nullptr;
+    int kron_cw = 0;
+    if (kron) {
+        if ((rc = kron_check(kron))) return rc;
+        EDX_REQUIRE(kron->nrows == n, "edx_krylov: apply_kron describes %lld rows, the matrix has %lld",
+                    (long long)kron->nrows, (long long)n);
+        EDX_REQUIRE(!packed, "edx_krylov: give apply_packed or apply_kron, not both");
+        kron_cw = kron_col_group(k, opts->apply_col_group);
+    }
     const int kw = pow2_kw(k);  // layout of the element-wise recurrence kernels
     const int gy = (k + kw - 1) / kw;
     int gx = num_sms() * 8;
+    if (kron) gx = std::max(gx, kron_grid_x(kron, k, kron_cw));
     Workspace w(d_work, work_bytes);
     KrylovWs ws;
     krylov_layout(w, n, k, nshift, maxn, gx, &ws);
@@ -956,6 +940,15 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     S.k = k;
 
     EDX_CUDA(cudaMemsetAsync(ws.ticket, 0, 4 * sizeof(unsigned), st));
+    EDX_CUDA(cudaMemsetAsync(ws.kticket, 0, sizeof(unsigned) * (size_t)k, st));
+    EDX_CUDA(cudaMemsetAsync(ws.kron_err, 0, sizeof(int), st));
+    // tensor maps of the two Lanczos blocks for the slab product's staged loads (they swap
+    // roles every step)
+    alignas(64) CUtensorMap tm_c, tm_p;
+    if (kron) {
+        if ((rc = kron_tensor_map(kron, ws.Vc, k, kron_cw, &tm_c))) return rc;
+        if ((rc = kron_tensor_map(kron, ws.Vp, k, kron_cw, &tm_p))) return rc;
+    }
     EDX_CUDA(cudaMemsetAsync(ws.gticket, 0, sizeof(unsigned) * (size_t)((k + 31) / 32), st));
     EDX_CUDA(cudaMemsetAsync(d_alpha, 0, sizeof(double) * (size_t)k * maxn, st));
     EDX_CUDA(cudaMemsetAsync(d_beta, 0, sizeof(double) * (size_t)k * maxn, st));
@@ -1037,7 +1030,10 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
             evs.push_back(e1);
             EDX_CUDA(cudaEventRecord(e0, st));
         }
-        if (packed)
+        if (kron)
+            rc = apply_kron(kron, Vc == ws.Vc ? static_cast<const void*>(&tm_c) : static_cast<const void*>(&tm_p), Vc,
+                            Vp, S, it, ws.kticket, ws.kron_err, kron_cw, st);
+        else if (packed)
             rc = apply_packed(packed, Vc, Vp, S, it, cfg, st);
         else
             rc = (A->val_type == EDX_C128) ? apply_v<double2>(A, Vc, Vp, S, it, cfg, st)
@@ -1062,9 +1058,13 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
         std::swap(Vc, Vp);
         if (it + 1 < maxn && (rc = project(Vc, it + 1))) return rc;
         if ((it + 1) % poll == 0 || it + 1 == maxn) {
-            int h[2] = {0, 0};
-            EDX_CUDA(cudaMemcpyAsync(h, ws.n_active, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            int h[3] = {0, 0, 0};
+            EDX_CUDA(cudaMemcpyAsync(h, ws.n_active, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
             EDX_CUDA(cudaStreamSynchronize(st));
+            if (h[2]) {
+                drop_events();
+                return fail(EDX_ERR_CUDA, "edx_krylov: a staged slab load did not arrive within its time limit");
+            }
             if (h[0] == 0) break;
             if (nshift > 0 && h[1] == 0) break;
         }

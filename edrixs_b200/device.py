@@ -12,7 +12,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import BuildDesc, Csr, KrylovOpts, Packed, call
+from ._lib import BuildDesc, Csr, KrylovOpts, Kron, Packed, call
 
 C128, C64 = _lib.EDX_C128, _lib.EDX_C64
 HAM_I, HAM_N, TRANS_I, TRANS_F = _lib.EDX_HAM_I, _lib.EDX_HAM_N, _lib.EDX_TRANS_I, _lib.EDX_TRANS_F
@@ -284,6 +284,128 @@ def pack(A: CSR, form="auto"):
 # products and solvers
 # ------------------------------------------------------------------------------------
 
+# ------------------------------------------------------------------------------------
+# slab form (edx_kron_*)
+# ------------------------------------------------------------------------------------
+
+KRON_SRC_HA, KRON_SRC_OWN, KRON_SRC_CRE, KRON_SRC_ANN = 0, 1, 2, 3
+
+
+@dataclass
+class KronMatrix:
+    """Device arrays of the slab form of a Hamiltonian (edrixs_b200/kron.py, include/edx.h
+    edx_kron); its rows and columns are in slab order.  perm[i] is the reference row of slab
+    row i, inv its inverse."""
+    spec: object
+    nrows: int
+    max_rows: int
+    t: dict
+    perm: torch.Tensor
+    inv: torch.Tensor
+
+    def desc(self):
+        t = self.t
+        return Kron(self.nrows, self.spec.nslab, self.spec.nb, self.spec.nah, self.spec.n_alo, self.max_rows,
+                    _ptr(t["slab_off"]), _ptr(t["slab_m"]), _ptr(t["slab_cfg"]), _ptr(t["hyb_a"]), _ptr(t["t_cre"]),
+                    _ptr(t["t_ann"]), _ptr(t["src_ptr"]), _ptr(t["src_slab"]), _ptr(t["src_kind"]),
+                    _ptr(t["src_coef"]), _ptr(t["b_off"]), _ptr(t["b_cfg"]), _ptr(t["b_nbr"]), _ptr(t["b_diag"]))
+
+    def shape_desc(self):
+        """A CSR descriptor with this matrix's shape and no entries, for edx_krylov with
+        apply_kron (the product runs on the slab form)."""
+        return Csr(self.nrows, self.nrows, 0, _ptr(self.t["slab_off"]), None, None, C128)
+
+    def nbytes(self):
+        return sum(x.numel() * x.element_size() for x in self.t.values()) + 16 * self.nrows
+
+    @property
+    def nnz(self):
+        return 0
+
+    def to_slab(self, X):
+        """Rows of X (reference order) in slab order."""
+        return permute_rows(X, self.perm)
+
+    def from_slab(self, X):
+        """Rows of X (slab order) in reference order."""
+        return permute_rows(X, self.inv)
+
+
+def kron_form(mode, basis: Basis, hopping, coulomb=None, num_val_orbs=0, num_core_orbs=0):
+    """The slab form of the Hamiltonian that build_csr(mode, basis, hopping, coulomb, ...)
+    builds (HAM_I, or HAM_N with ham_sign = +1), or None when the terms have no impurity x bath
+    structure.  H_A is built by the same bit-exact build on the A configurations."""
+    from . import kron
+    if mode not in (HAM_I, HAM_N):
+        return None
+    spec = kron.kron_spec(hopping, coulomb, basis.states.cpu().numpy(), "ham_i" if mode == HAM_I else "ham_n",
+                          num_val_orbs=num_val_orbs, num_core_orbs=num_core_orbs)
+    if spec is None:
+        return None
+    HA = build_csr(HAM_I, basis_from_states(spec.slab_full.astype(np.uint64)), spec.a_hop,
+                   spec.a_coul if len(spec.a_coul[1]) else None)
+    rp, col, val = HA.row_ptr.cpu().numpy(), HA.col.cpu().numpy(), HA.val.cpu().numpy()
+    # per-slab source list: the slab itself (H_A's diagonal + bath levels), H_A's other
+    # columns, then the slabs one bath electron away
+    has_cre = np.any(spec.t_cre != 0, axis=1)
+    has_ann = np.any(spec.t_ann != 0, axis=1)
+    ptr, sl, kind, coef = [0], [], [], []
+    for s in range(spec.nslab):
+        j0, j1 = rp[s], rp[s + 1]
+        cs, vs = col[j0:j1], val[j0:j1]
+        d = vs[cs == s]
+        sl.append(s)
+        kind.append(KRON_SRC_OWN)
+        coef.append(d[0] if len(d) else 0j)
+        off = cs != s
+        sl.extend(cs[off].tolist())
+        kind.extend([KRON_SRC_HA] * int(off.sum()))
+        coef.extend(vs[off].tolist())
+        for q in range(spec.nah):
+            u, dn = spec.up[s, q], spec.dn[s, q]
+            if u >= 0 and has_cre[q]:
+                sl.append(int(u))
+                kind.append(KRON_SRC_CRE | (q << 4))
+                coef.append(0j)
+            if dn >= 0 and has_ann[q]:
+                sl.append(int(dn))
+                kind.append(KRON_SRC_ANN | (q << 4))
+                coef.append(0j)
+        ptr.append(len(sl))
+    dev = dict(device="cuda")
+
+    def i32(a):
+        return torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64).astype(np.int32), **dev)
+
+    def c128(a):
+        return torch.as_tensor(np.ascontiguousarray(a, dtype=np.complex128).reshape(-1), **dev)
+
+    def u16(a):
+        return torch.as_tensor(np.ascontiguousarray(a, dtype=np.uint16).reshape(-1).view(np.int16), **dev)
+
+    t = dict(slab_off=i32(spec.slab_off), slab_m=i32(spec.slab_m), slab_cfg=i32(spec.slab_cfg),
+             hyb_a=i32(spec.hyb_a if spec.nah else [0]), t_cre=c128(spec.t_cre if spec.nah else [0j]),
+             t_ann=c128(spec.t_ann if spec.nah else [0j]),
+             src_ptr=torch.as_tensor(np.asarray(ptr, dtype=np.int64), **dev), src_slab=i32(sl), src_kind=i32(kind),
+             src_coef=c128(coef), b_off=i32(spec.b_off), b_cfg=u16(spec.b_cfg), b_nbr=u16(spec.b_nbr),
+             b_diag=c128(spec.b_diag))
+    perm = torch.as_tensor(spec.perm, dtype=torch.int64, **dev)
+    inv = torch.empty_like(perm)
+    inv[perm] = torch.arange(spec.n, dtype=torch.int64, **dev)
+    return KronMatrix(spec, spec.n, spec.max_rows, t, perm, inv)
+
+
+def permute_rows(X, idx):
+    """Y[i] = X[idx[i]] (rows of a complex128 block), by libedx's edx_permute_rows."""
+    Xm = X.reshape(X.shape[0], -1)
+    if Xm.stride(1) != 1 and Xm.shape[1] > 1:
+        Xm = Xm.contiguous()
+    n, k = idx.numel(), Xm.shape[1]
+    Y = torch.empty((n, k), dtype=torch.complex128, device=X.device)
+    call("edx_permute_rows", n, k, _ptr(Xm), Xm.stride(0), _ptr(idx), _ptr(Y), k, _stream())
+    return Y.reshape(-1) if X.dim() == 1 else Y
+
+
 def spmm(A, X, Y=None, alpha=1.0, sigma=0.0, beta=0.0, c64=False, col_group=0):
     """Y = alpha*(A X) + sigma*X + beta*Y; X is (ncols,) or (ncols, k) row-major.  A is a CSR
     or a PackedMatrix (edx_spmm_packed)."""
@@ -302,7 +424,15 @@ def spmm(A, X, Y=None, alpha=1.0, sigma=0.0, beta=0.0, c64=False, col_group=0):
     if k > 1 and Ym.stride(1) != 1:
         raise ValueError("spmm: Y must be row-major (n, k)")
     al, sg, be = complex(alpha), complex(sigma), complex(beta)
-    if isinstance(A, PackedMatrix):
+    if isinstance(A, KronMatrix):
+        if vec_type != C128 or c64 or al != 1 or sg != 0 or be != 0 or Xm.stride(0) != k or Ym.stride(0) != k:
+            raise ValueError("spmm: the slab form computes Y = H X on contiguous complex128 blocks only")
+        ws = ctypes.c_size_t(0)
+        call("edx_kron_spmm_workspace", ctypes.byref(ws))
+        w = _work(ws.value)
+        call("edx_kron_spmm", ctypes.byref(A.desc()), k, _ptr(Xm), _ptr(Ym), col_group, _ptr(w), ws.value,
+             _stream())
+    elif isinstance(A, PackedMatrix):
         if vec_type != C128 or c64:
             raise ValueError("spmm: a packed matrix takes complex128 vectors")
         call("edx_spmm_packed", ctypes.byref(A.desc()), k, _ptr(Xm), Xm.stride(0), _ptr(Ym), Ym.stride(0),
@@ -337,6 +467,8 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
     only the last B projected vectors."""
     if isinstance(A, PackedMatrix):
         apply = dict(apply or {}, packed=A)
+    if isinstance(A, KronMatrix):
+        apply = dict(apply or {}, kron=A)
     kcols = V0.reshape(V0.shape[0], -1).shape[1]
     if apply and apply.get("packed") is not None and "rowslot" not in apply and kcols <= 16 \
             and "col_group" not in apply:
@@ -418,6 +550,10 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
             pdesc = apply["packed"].desc()
             opts.apply_packed = ctypes.pointer(pdesc)
             keep += [pdesc]
+        if apply.get("kron") is not None:
+            kdesc = apply["kron"].desc()
+            opts.apply_kron = ctypes.pointer(kdesc)
+            keep += [kdesc]
     ms = ctypes.c_double(0.0)
     nl = ctypes.c_int(0)
     if timing:
@@ -426,7 +562,7 @@ def krylov(A, V0, maxn, c64=False, proj=(), shifts=None, shift_tol=1e-10, shift_
     ws = ctypes.c_size_t(0)
     call("edx_krylov_workspace", n, k, ctypes.byref(opts), maxn, ctypes.byref(ws))
     w = _work(ws.value)
-    adesc = A.shape_desc() if isinstance(A, PackedMatrix) else A.desc(c64)
+    adesc = A.shape_desc() if isinstance(A, (PackedMatrix, KronMatrix)) else A.desc(c64)
     call("edx_krylov", ctypes.byref(adesc), k, _ptr(V0), maxn, _ptr(alpha), _ptr(beta), _ptr(norm),
          _ptr(neff), ctypes.byref(opts), _ptr(w), ws.value, _stream())
     # projected vectors exist for v_0 .. v_L after L iterations

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define EDX_ABI_VERSION 4
+#define EDX_ABI_VERSION 5
 
 /* status codes */
 #define EDX_OK 0
@@ -181,6 +181,65 @@ int edx_spmm_packed(const edx_packed* P, int k, const double* d_x, int64_t ldx, 
                     double beta_im, int col_group, void* stream);
 
 /* ---------------------------------------------------------------------------------- */
+/* Slab form of an impurity-model Hamiltonian (no counterpart in the reference, whose     */
+/* matvec_csr src/spmv.f90:73-103 walks a flat CSR built by src/ham.f90:2-711)          */
+/* ---------------------------------------------------------------------------------- */
+
+/* When the two-body terms touch only the "A" orbitals (impurity and core) and the bath
+ * orbitals carry only their levels and the A-bath hybridisation, every Fock state is a pair
+ * (I, B) of an A configuration and a bath configuration, and
+ *   H = H_A (x) 1 + diag(d_B) + sum_{a,b} t_cre[a][b] c+_a c_b + t_ann[a][b] c+_b c_a.
+ * Rows are grouped by I into slabs (slab s = rows slab_off[s] .. slab_off[s+1]-1, its bath
+ * configurations in colex order of sector slab_m[s]), so the product reads whole source
+ * slabs: those of H_A's row s, and the slabs I +- a one bath electron away.  Rows here are in
+ * slab order; the host keeps the permutation to the reference's row order.  Built on the host
+ * (edrixs_b200/kron.py) from the term lists; bath tables index b_off[m] + rank.  Signs:
+ * A-side factors come from the compressed A configuration slab_cfg[s] (A orbitals numbered
+ * by ascending full-state bit, the n_alo below the bath first), bath-side factors from the
+ * bath configuration; the formulas are in edrixs_b200/kron.py. */
+#define EDX_KRON_NB_MAX 16
+#define EDX_KRON_NAH_MAX 16
+/* source kinds of slab s (src_kind = kind | q << 4) */
+#define EDX_KRON_SRC_HA 0    /* another slab of H_A's row s: Y += coef X_src */
+#define EDX_KRON_SRC_OWN 1   /* slab s itself: Y += (coef + b_diag[B]) X_s (coef = H_A's diagonal) */
+#define EDX_KRON_SRC_CRE 2   /* slab I + a_q: Y(B) += sum_{b in B} sign t_cre[q][b] X_src(B - b) */
+#define EDX_KRON_SRC_ANN 3   /* slab I - a_q: Y(B) += sum_{b not in B} sign t_ann[q][b] X_src(B + b) */
+typedef struct edx_kron {
+    int64_t nrows;
+    int32_t nslab, nb, nah, n_alo;
+    int32_t max_rows;           /* rows of the largest slab */
+    const int32_t* slab_off;    /* device int32[nslab+1] */
+    const int32_t* slab_m;      /* device int32[nslab] bath electrons */
+    const uint32_t* slab_cfg;   /* device uint32[nslab] compressed A configuration */
+    const int32_t* hyb_a;       /* device int32[nah]: compressed A index a_q */
+    const double* t_cre;        /* device complex128[nah*nb]: coefficient of c+_{a_q} c_b */
+    const double* t_ann;        /* device complex128[nah*nb]: coefficient of c+_b c_{a_q} */
+    const int64_t* src_ptr;     /* device int64[nslab+1]: sources of slab s, own slab first */
+    const int32_t* src_slab;    /* device int32[nsrc] */
+    const int32_t* src_kind;    /* device int32[nsrc] */
+    const double* src_coef;     /* device complex128[nsrc] (H_A entries; 0 for CRE / ANN) */
+    const int32_t* b_off;       /* device int32[nb+2] */
+    const uint16_t* b_cfg;      /* device uint16[2^nb] */
+    const uint16_t* b_nbr;      /* device uint16[2^nb * nb]: rank of cfg ^ (1 << x) in its sector */
+    const double* b_diag;       /* device complex128[2^nb] */
+} edx_kron;
+
+/* Y = H X in slab order for k columns (row-major, ld = k), on the slab form.  The source
+ * slabs are staged in shared memory by the tensor-memory accelerator (2-D tiled loads of
+ * 32-row boxes; no multicast).  col_group: columns per block (1, 2, 4, 6, 8, 12 or 16;
+ * 0 = the smallest >= k, 16 beyond).  EDX_ERR_CUDA if a staged load did not arrive within
+ * its time limit (the kernel records it in the workspace).  X and Y must not overlap. */
+int edx_kron_spmm_workspace(size_t* bytes);
+int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double* d_y, int col_group, void* d_work,
+                  size_t work_bytes, void* stream);
+
+/* dst[i*ld_dst + c] = src[idx[i]*ld_src + c] for i < n, c < k (complex128): moves blocks
+ * between the reference's row order and the slab order (idx = the permutation, or its
+ * inverse). */
+int edx_permute_rows(int64_t n, int k, const double* d_src, int64_t ld_src, const int64_t* d_idx, double* d_dst,
+                     int64_t ld_dst, void* stream);
+
+/* ---------------------------------------------------------------------------------- */
 /* Block Gram-Schmidt for the ground-state eigensolver (the reorthogonalisation inside      */
 /* ARPACK's pznaupd, src/arpack.f90:76, done here for the thick-restart Lanczos)          */
 /* ---------------------------------------------------------------------------------- */
@@ -250,6 +309,10 @@ typedef struct edx_krylov_opts {
      * one 32-bit word per off-diagonal entry and the value from a table in shared memory,
      * with the launch-shape fields above. */
     const edx_packed* apply_packed;
+    /* slab form of the same matrix, or NULL.  With it the product is k_lanczos_apply_kron:
+     * the start vectors d_v0 and every Lanczos vector are in slab order, and A is used for
+     * its shape only.  Projections need operators whose columns are in slab order too. */
+    const edx_kron* apply_kron;
     /* streaming projections, for problems where P_p V (every projected Lanczos vector) does
      * not fit in memory.  With proj_window = B > 0, proj_out[p] holds only the last B
      * projected vectors (device complex128[k][B][nrows_p]) and every B iterations (and at

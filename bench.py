@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-packed", action="store_true", help="no packed forms of H_n, H_f (CSR products only)")
+    ap.add_argument("--no-kron", action="store_true", help="no slab (impurity x bath) forms of H_n, H_f")
     ap.add_argument("--ed", action="store_true",
                     help="plain FP64 ED instead of RIXS: lowest eigenpairs of a 10 + 14 orbital model")
     ap.add_argument("--ed-nbath", type=int, default=14)
@@ -254,11 +255,19 @@ def setup_gpu(args, ngs=3):
             pm = device.pack(M)
             if pm is not None:
                 packed[name] = pm
+    kron = {}
+    if not args.no_kron and not args.c64:
+        for name, mode, b, hop, coul, nc in (("hf", device.HAM_I, bi, t["hop_i"], t["coul_i"], 0),
+                                             ("hn", device.HAM_N, bn, t["hop_n"], t["coul_n"], 6)):
+            K = device.kron_form(mode, b, hop, coul, num_val_orbs=nv, num_core_orbs=nc)
+            if K is not None:
+                kron[name] = K
     gs_e, gs_v = solvers.lowest_eigs(Hf, ngs, ngs, tol=1e-9, packed=packed.get("hf"))
     e_n, _ = solvers.lowest_eigs(Hn, 1, 1, tol=1e-6, packed=packed.get("hn"))
     edge = float(e_n[0] - gs_e[0])
     P = rixs.RixsProblem(Hn=Hn, Hf=Hf, Din=Din, Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v.contiguous())
     P.packed.update(packed)
+    P.kron.update(kron)
     omegas = edge - 2.0 + np.linspace(0.0, 10.0, args.n_omega)
     eloss = np.linspace(-0.5, 12.0, args.n_eloss)
     torch.cuda.synchronize()
@@ -578,9 +587,14 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     st = stats[-1]
 
-    def roof(nnz, rows, k, ms, launches, c64, packed=None):
+    def roof(nnz, rows, k, ms, launches, c64, packed=None, kron=None):
         sv = 8 if c64 else 16
-        if packed is not None:
+        if kron is not None:
+            # the slab product streams no matrix: V_cur once, V_prev read and written, and the
+            # slab, source and bath tables
+            tables = sum(x.numel() * x.element_size() for x in kron.t.values())
+            per_launch = tables + 3 * k * rows * 16
+        elif packed is not None:
             # what the packed product must read once: entry words, row pointers, diagonal, table
             per_launch = (packed.ent.numel() * 4 + (rows + 1) * 8 + rows * 16 + packed.vals.numel() * 16
                           + 3 * k * rows * 16)
@@ -593,17 +607,19 @@ def run_ours(args):
                     launches=launches, total_ms=round(ms, 3))
 
     r_hf = roof(st["hf_nnz"], st["hf_rows"], st["k_hf"], st["hf_apply_ms"], st["hf_iterations"], args.c64,
-                P.packed.get("hf") if st.get("hf_packed") else None)
+                P.packed.get("hf") if st.get("hf_packed") else None, P.kron.get("hf") if st.get("hf_kron") else None)
     r_hn = roof(st["hn_nnz"], st["hn_rows"], st["k_hn"], st["hn_apply_ms"], st["hn_iterations"], args.c64,
-                P.packed.get("hn") if st.get("hn_packed") else None)
+                P.packed.get("hn") if st.get("hn_packed") else None, P.kron.get("hn") if st.get("hn_kron") else None)
     dom, sec = (r_hf, r_hn) if r_hf["total_ms"] >= r_hn["total_ms"] else (r_hn, r_hf)
 
-    def kname(packed, cfg):
+    def kname(packed, kron, cfg):
+        if kron:
+            return "k_lanczos_apply_kron"
         rs = bool(cfg and cfg.get("rowslot"))
         return ("k_lanczos_apply_packed" if packed else "k_lanczos_apply") + ("_rs" if rs else "")
 
-    hf_kernel = kname(st.get("hf_packed"), tuned.get(f"hf_k{st['k_hf']}"))
-    hn_kernel = kname(st.get("hn_packed"), tuned.get(f"hn_k{st['k_hn']}"))
+    hf_kernel = kname(st.get("hf_packed"), st.get("hf_kron"), tuned.get(f"hf_k{st['k_hf']}"))
+    hn_kernel = kname(st.get("hn_packed"), st.get("hn_kron"), tuned.get(f"hn_k{st['k_hn']}"))
     # DRAM traffic of the launch shape that ran, from an ncu capture of exactly that launch
     for r, kern, cfg_key, k_, rows_ in ((r_hf, hf_kernel, f"hf_k{st['k_hf']}", st["k_hf"], st["hf_rows"]),
                                         (r_hn, hn_kernel, f"hn_k{st['k_hn']}", st["k_hn"], st["hn_rows"])):

@@ -342,8 +342,9 @@ def kron_form(mode, basis: Basis, hopping, coulomb=None, num_val_orbs=0, num_cor
                           num_val_orbs=num_val_orbs, num_core_orbs=num_core_orbs)
     if spec is None:
         return None
+    # rows are A configurations as full-state bit patterns (valence and core bits in place)
     HA = build_csr(HAM_I, basis_from_states(spec.slab_full.astype(np.uint64)), spec.a_hop,
-                   spec.a_coul if len(spec.a_coul[1]) else None)
+                   spec.a_coul if len(spec.a_coul[1]) else None, num_val_orbs=num_val_orbs + num_core_orbs)
     rp, col, val = HA.row_ptr.cpu().numpy(), HA.col.cpu().numpy(), HA.val.cpu().numpy()
     # per-slab source list: the slab itself (H_A's diagonal + bath levels), H_A's other
     # columns, then the slabs one bath electron away
@@ -393,6 +394,15 @@ def kron_form(mode, basis: Basis, hopping, coulomb=None, num_val_orbs=0, num_cor
     inv = torch.empty_like(perm)
     inv[perm] = torch.arange(spec.n, dtype=torch.int64, **dev)
     return KronMatrix(spec, spec.n, spec.max_rows, t, perm, inv)
+
+
+def relabel_columns(D: CSR, idx):
+    """D with column j renamed idx[j] (row pointers and values shared): an operator whose
+    columns were in the reference's row order of a matrix, re-expressed on that matrix's slab
+    order (idx = KronMatrix.inv).  Rows keep their entry order, so each row's sum is taken in
+    the same order as on D."""
+    col = idx.index_select(0, D.col.to(torch.int64)).to(torch.int32)
+    return CSR(D.row_ptr, col, D.val, D.ncols, D.val64)
 
 
 def permute_rows(X, idx):

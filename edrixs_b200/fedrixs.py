@@ -60,8 +60,14 @@ def ed_core(cfg, H):
     if ed_solver == 0:
         e, v = solvers.dense_eigs(H, max(neval, nvector))
         return e[:neval], v[:, :nvector]
+    if ed_solver == 1:
+        # the reference's plain Lanczos (src/lanczos.f90:6-167): its stopping rule, and on a
+        # degenerate spectrum its lowest distinct levels
+        return solvers.plain_lanczos_eigs(H, neval, nvector, cfg["maxiter"], float(cfg["eigval_tol"]),
+                                          packed=device.pack(H))
     tol = min(float(cfg["eigval_tol"]), 1e-9)
-    # products on the packed form when H has few enough distinct values (lossless)
+    # ARPACK's place (src/arpack.f90:2-112): block thick-restart Lanczos; products on the
+    # packed form when H has few enough distinct values (lossless)
     e, v = solvers.lowest_eigs(H, neval, nvector, tol=tol, packed=device.pack(H))
     return e, v
 

@@ -52,24 +52,42 @@ class RixsProblem:
     gs_v: torch.Tensor                       # (n_i, ngs) complex128
     meta: dict = field(default_factory=dict)
     packed: dict = field(default_factory=dict)  # "hf" / "hn" -> device.PackedMatrix of that matrix
+    kron: dict = field(default_factory=dict)    # "hf" / "hn" -> device.KronMatrix (slab form) of that matrix
 
     def nbytes(self):
         b = self.Hn.nbytes() + self.Hf.nbytes() + sum(D.nbytes() for D in self.Din + self.Dout)
         if self.Hn.val64 is not None:
             b += self.Hn.nnz * 8
         b += sum(M.nbytes() for M in self.packed.values())
+        b += sum(M.nbytes() for M in self.kron.values())
         return b + self.gs_v.numel() * 16
 
+    def dout_on_slabs(self):
+        """D_out with its columns in the slab order of H_n (for projecting Lanczos vectors that
+        live in that order); built once and kept."""
+        key = ("dout_slab", id(self.kron["hn"]))
+        if key not in self.meta:
+            inv = self.kron["hn"].inv
+            self.meta[key] = [device.relabel_columns(D, inv) for D in self.Dout]
+        return self.meta[key]
 
-def _apply_args(cfg, packed, c64):
-    """Launch arguments of one Krylov call: the autotuner's choice, else the packed product
-    when a packed form exists, else libedx's defaults."""
+
+def _apply_args(cfg, packed, c64, kron=None):
+    """Launch arguments of one Krylov call: the autotuner's choice, else the slab product when
+    a slab form exists, else the packed product when a packed form exists, else libedx's
+    defaults."""
     if cfg is not None:
+        if cfg.get("kron"):
+            if kron is None:
+                raise ValueError("the tuned launch shape needs the slab form")
+            return dict(col_group=cfg.get("col_group", 0), kron=kron)
         if cfg.get("packed"):
             if packed is None:
                 raise ValueError("the tuned launch shape needs the packed form")
             return dict(cfg, packed=packed)
         return cfg
+    if kron is not None and not c64:
+        return dict(kron=kron)
     if packed is not None and not c64:
         return dict(packed=packed)
     return None
@@ -120,16 +138,24 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     K_hf = npout * k_hn * n_om if final_block is None else int(final_block)
     if autotune:
         from . import tune
-        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64, packed=P.packed.get("hn"))
-        P.meta[("apply", "hf", K_hf, c64_f)] = tune.tune_apply(P.Hf, K_hf, c64=c64_f, packed=P.packed.get("hf"))
-    cfg_hn = _apply_args(P.meta.get(("apply", "hn", k_hn, c64)), P.packed.get("hn"), c64)
-    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64_f)), P.packed.get("hf"), c64_f)
+        P.meta[("apply", "hn", k_hn, c64)] = tune.tune_apply(P.Hn, k_hn, c64=c64, packed=P.packed.get("hn"),
+                                                             kron=P.kron.get("hn"))
+        P.meta[("apply", "hf", K_hf, c64_f)] = tune.tune_apply(P.Hf, K_hf, c64=c64_f, packed=P.packed.get("hf"),
+                                                               kron=P.kron.get("hf"))
+    cfg_hn = _apply_args(P.meta.get(("apply", "hn", k_hn, c64)), P.packed.get("hn"), c64, P.kron.get("hn"))
+    cfg_hf = _apply_args(P.meta.get(("apply", "hf", K_hf, c64_f)), P.packed.get("hf"), c64_f, P.kron.get("hf"))
+    # on the slab form of H_n the Lanczos vectors are in its slab order: seeds go in permuted,
+    # and D_out^+ reads them through columns relabelled to that order
+    Kn = cfg_hn.get("kron") if cfg_hn else None
+    Kf = cfg_hf.get("kron") if cfg_hf else None
+    dout = P.dout_on_slabs() if Kn is not None else P.Dout
     gam_c = np.broadcast_to(np.asarray(gamma_c, dtype=np.float64), (n_om,))
     dev = P.gs_v.device
     # 1. seeds (n_n, npin*ngs), column c = p_in*ngs + g
     if seeds is None:
         seeds = torch.cat([device.spmm(D, P.gs_v) for D in P.Din], dim=1).contiguous()
     k = seeds.shape[1]
+    seeds_k = Kn.to_slab(seeds) if Kn is not None else seeds
     # 2. shifts: for every column its n_om incident energies
     scol = np.repeat(np.arange(k, dtype=np.int32), n_om)
     gsE = np.tile(P.gs_e, npin)
@@ -141,10 +167,10 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     K = npout * k * n_om
     # 3. one Krylov space per seed + projections through every D_out^+
     if not stream:
-        r = device.krylov(P.Hn, seeds, maxn, c64=c64, proj=P.Dout, shifts=(scol, sz), shift_tol=linsys_tol,
+        r = device.krylov(P.Hn, seeds_k, maxn, c64=c64, proj=dout, shifts=(scol, sz), shift_tol=linsys_tol,
                           shift_maxit=linsys_max, timing=timing, apply=cfg_hn)
     else:  # pass 1: the shifted recurrences alone
-        r = device.krylov(P.Hn, seeds, maxn, c64=c64, shifts=(scol, sz), shift_tol=linsys_tol,
+        r = device.krylov(P.Hn, seeds_k, maxn, c64=c64, shifts=(scol, sz), shift_tol=linsys_tol,
                           shift_maxit=linsys_max, timing=timing, apply=cfg_hn)
     steps = int(r.neff.max().item())
     m = max(int(r.shift_iters.max().item()), 1)
@@ -154,7 +180,8 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     # libedx launches on H_n: 4 setup + the first projections, then per iteration apply, orth,
     # shift step and per emission operator a projection and its column scaling
     stats = dict(hn_iterations=it_n, hn_apply_ms=r.apply_ms, hn_nnz=P.Hn.nnz, hn_rows=P.Hn.nrows, k_hn=k,
-                 launches=npin + 4 + npout + it_n * (3 + 2 * npout), streamed=bool(stream))
+                 launches=npin + 4 + npout + it_n * (3 + 2 * npout) + (Kn is not None) + (Kf is not None),
+                 streamed=bool(stream))
     if not stream:
         Y = r.shift_y.view(k, n_om, -1)[:, :, :m]                 # (k, n_om, m)
         # phi[p_out][c, w, :] = sum_i Y[c, w, i] * (D_out^+ v_i)[:]
@@ -175,7 +202,7 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
         V0 = torch.zeros((nf, K), dtype=torch.complex128, device=dev)
         nacc = k * n_om
         outs = [V0[:, po * nacc:(po + 1) * nacc] for po in range(npout)]
-        r2 = device.krylov(P.Hn, seeds, m, c64=c64, proj=P.Dout, timing=timing, apply=cfg_hn,
+        r2 = device.krylov(P.Hn, seeds_k, m, c64=c64, proj=dout, timing=timing, apply=cfg_hn,
                            accumulate=dict(window=int(stream_window), col=scol, coef=Y, out=outs))
         stats["hn_iterations"] += r2.apply_launches
         if timing:
@@ -184,6 +211,8 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
             npout * ((m + int(stream_window) - 1) // int(stream_window))
         del r2, Y
     start = V0[:, list(start_cols)].clone() if start_cols is not None else None
+    if Kf is not None:  # the final-state Lanczos runs in the slab order of H_f
+        V0 = Kf.to_slab(V0)
     # 4. final-state Lanczos, all pole sets as one block (optionally in chunks of columns)
     blk = K if final_block is None else int(final_block)
     A = torch.zeros((K, nkryl), dtype=torch.float64, device=dev)
@@ -201,7 +230,8 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
     stats.update(hf_apply_ms=hf_ms if timing else None, hf_iterations=hf_it, hf_nnz=P.Hf.nnz, hf_rows=P.Hf.nrows,
                  k_hf=blk,
                  hf_packed=bool(cfg_hf and cfg_hf.get("packed") is not None),
-                 hn_packed=bool(cfg_hn and cfg_hn.get("packed") is not None))
+                 hn_packed=bool(cfg_hn and cfg_hn.get("packed") is not None),
+                 hf_kron=Kf is not None, hn_kron=Kn is not None)
     del V0
     # 5. continued fractions; column order (p_out, p_in, g, w)
     e0 = np.tile(np.repeat(np.tile(P.gs_e, npin), n_om), npout)

@@ -148,3 +148,86 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
     U = (Yv.T @ V[:m]).T.contiguous()          # n x nvec
     U = U / torch.linalg.vector_norm(U, dim=0, keepdim=True)
     return theta[:nev].copy(), U
+
+
+def _plain_replay(a, b, neff, computed, nev, max_niter, eval_tol):
+    """The stopping logic of diag_ham_lanczos (src/lanczos.f90:76-131) replayed on Lanczos
+    coefficients already computed: a[i-1] = alpha_i, b[i-1] = beta_i for i <= neff, where the
+    device recurrence ran `computed` steps (neff < computed means beta_neff < 1e-10).  Every
+    10th step and at max_niter the eigenvalues of T_i are taken (dsteqr, :169-206); once
+    i >= nev the run stops when the nev-th one moved by less than eval_tol since the last
+    check (the first check compares with 0).  Returns (evals[nev], ritz vectors of T_i, nkrylov),
+    nkrylov = 0 when max_niter passes without convergence (the reference's eigenvectors are
+    then zero), or None when more steps than were computed are needed."""
+    from scipy.linalg import lapack
+
+    def tri(i):
+        d, z, info = lapack.dstev(np.asarray(a[:i], dtype=np.float64), np.asarray(b[:i - 1], dtype=np.float64),
+                                  compute_v=1)
+        if info != 0:
+            raise RuntimeError(f"dstev info {info}")
+        return np.concatenate([d, np.zeros(max(0, nev - i))]), z
+
+    evals = np.zeros(nev)
+    for i in range(1, max_niter + 1):
+        if i > neff:
+            return None  # the device recurrence has to run further
+        if i % 10 == 0 or i == max_niter:
+            ke, kv = tri(i)
+            if i >= nev and abs(ke[nev - 1] - evals[nev - 1]) < eval_tol:
+                return ke[:nev].copy(), kv, i
+            evals = ke[:nev].copy()
+        broke = neff < computed and i == neff
+        if broke:  # beta_i < 1e-10: the Krylov space is exhausted
+            if i >= 2:
+                ke, kv = tri(i)
+                evals = ke[:nev].copy()
+            else:
+                evals[0] = a[0]
+                kv = np.ones((1, 1))
+            return evals, kv, i
+    return evals, None, 0
+
+
+def plain_lanczos_eigs(H, nev, nvec, max_niter, eval_tol, seed=0, packed=None):
+    """diag_ham_lanczos (src/lanczos.f90:6-167), the ed_solver = 1 path of
+    src/ed_driver.f90:154-158, on the device.
+
+    Plain Lanczos without reorthogonalisation, as the reference runs it: the start vector is
+    uniform reals in [-0.5, 0.5), normalised (:60-70; seeded here, the reference's is not),
+    and the coefficients come from libedx's recurrence (edx_krylov, one column, the
+    reference's breakdown rule beta < 1e-10).  The stopping rule is replayed on them on the
+    host (_plain_replay), running the device recurrence further (twice as many steps) until
+    the rule decides.  Eigenvectors: the recurrence is run again for nkrylov steps and
+    sum_i z_ij v_i accumulated on the device (:133-157), through an identity projection
+    folded into accumulators.  On a degenerate spectrum the Krylov space holds one direction
+    per distinct level, so the eigenvalues are the lowest distinct levels, as the reference
+    reports them.  Returns (evals[nev] host array, evecs (n, nvec) device tensor)."""
+    n = H.nrows
+    rng = np.random.default_rng(seed)
+    v1 = (rng.random(n) - 0.5).astype(np.complex128)
+    v1 /= np.sqrt(np.vdot(v1, v1).real)
+    V0 = torch.from_numpy(v1).to("cuda").reshape(-1, 1).contiguous()
+    apply = dict(packed=packed) if packed is not None else None
+    m = min(int(max_niter), 64)
+    while True:
+        r = device.krylov(H, V0, m, apply=apply)
+        neff = int(r.neff[0].item())
+        got = _plain_replay(r.alpha[0, :neff].cpu().numpy(), r.beta[0, :neff].cpu().numpy(), neff, m, nev,
+                            int(max_niter), eval_tol)
+        if got is not None:
+            break
+        m = min(int(max_niter), 2 * m)
+    evals, kv, nk = got
+    out = torch.zeros((n, nvec), dtype=torch.complex128, device="cuda")
+    if nk > 0 and nvec > 0:
+        q = min(nvec, kv.shape[1])
+        coef = torch.zeros((nvec, nk), dtype=torch.complex128, device="cuda")
+        coef[:q] = torch.from_numpy(np.ascontiguousarray(kv[:nk, :q].T)).to("cuda")
+        eye = device.CSR(torch.arange(n + 1, dtype=torch.int64, device="cuda"),
+                         torch.arange(n, dtype=torch.int32, device="cuda"),
+                         torch.ones(n, dtype=torch.complex128, device="cuda"), n)
+        device.krylov(H, V0, nk, proj=[eye], apply=apply,
+                      accumulate=dict(window=min(8, nk), col=np.zeros(nvec, dtype=np.int32), coef=coef.contiguous(),
+                                      out=[out]))
+    return evals, out

@@ -36,10 +36,19 @@ def candidates(k):
     return out
 
 
-def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, packed=None):
-    """Fastest launch shape for k columns on A.  With a packed form of A (complex128 only)
-    its products are timed too; the result then carries "packed": 1."""
-    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64), packed is not None)
+def kron_candidates(k):
+    """Columns per block of the slab product worth timing for k columns."""
+    if k > 16:
+        return [16, 8]
+    first = next(w for w in (1, 2, 4, 6, 8, 12, 16) if w >= k)
+    return sorted({first, min(16, 2 * first) if first < 16 else 16})
+
+
+def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, packed=None, kron=None):
+    """Fastest launch shape for k columns on A.  With a packed form or a slab form of A
+    (complex128 only) their products are timed too; the result then carries "packed": 1 or
+    "kron": 1."""
+    key = (A.row_ptr.data_ptr(), A.nnz, k, bool(c64), packed is not None, kron is not None)
     if key in _cache:
         return _cache[key]
     dev = A.row_ptr.device
@@ -56,7 +65,12 @@ def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, packed=None)
         cands = cands + [dict(c, packed=1, rowslot=0) for c in candidates(k)]
         if k <= 16:  # one row per lane group
             cands += [dict(c, packed=1, rowslot=1) for c in candidates(k) if c["chunked"] == 0]
+    if kron is not None and not c64:
+        cands = cands + [dict(kron=1, col_group=cw) for cw in kron_candidates(k)]
+
     def args_of(cfg):
+        if cfg.get("kron"):
+            return dict(col_group=cfg["col_group"], kron=kron)
         if cfg.get("packed"):
             return dict(cfg, packed=packed)
         return cfg

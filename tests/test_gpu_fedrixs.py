@@ -67,6 +67,62 @@ def test_ed_known_answer(cuda, golden_dir, workdir):
     assert os.path.exists("eigvec.45")
 
 
+def _set_config(path, **kw):
+    """Rewrite config.in entries key=value (as a namelist line each)."""
+    import re
+    txt = open(path).read()
+    for k, v in kw.items():
+        if re.search(rf"^\s*{k}\s*=", txt, flags=re.M | re.I):
+            txt = re.sub(rf"^(\s*){k}\s*=.*$", rf"\g<1>{k} = {v}", txt, flags=re.M | re.I)
+        else:
+            txt = re.sub(r"^(\s*&control.*)$", rf"\1\n{k} = {v}", txt, count=1, flags=re.M | re.I)
+    open(path, "w").write(txt)
+
+
+def test_ed_solver1_plain_lanczos_known_answer(cuda, golden_dir, workdir):
+    """ed_solver = 1 above min_ndim (src/ed_driver.f90:154-158): the drop-in runs the
+    reference's plain Lanczos (src/lanczos.f90:6-167), whose Krylov space holds one direction
+    per distinct level, so eigvals.dat lists the lowest DISTINCT levels of the 45-state known
+    answer, as the oracle's step-for-step restatement does; the eigenvectors are eigenvectors."""
+    from edrixs_b200 import fedrixs
+    from oracle import drivers
+    for f in os.listdir(os.path.join(golden_dir, "known_answer")):
+        shutil.copy(os.path.join(golden_dir, "known_answer", f), workdir)
+    _set_config("config.in", ed_solver=1, min_ndim=10, neval=3, nvector=3)
+    fedrixs.ed_fsolver(0, 0, 1)
+    _, e = np.loadtxt("eigvals.dat", unpack=True)
+    e_o, v_o, H, fock, cfg = drivers.ed(str(workdir), follow_ed_solver=True)
+    assert cfg["ed_solver"] == 1 and len(e) == 3
+    assert np.abs(e - e_o).max() < 1e-9  # the file carries 10 decimals
+    expected = np.loadtxt("expected_eigvals.txt")
+    levels = expected[np.r_[True, np.diff(expected) > 1e-8]]
+    assert np.abs(e - levels[:3]).max() < 1e-9
+    Hd = H.dense()
+    for k in range(3):
+        ek, vk = drivers.read_eigvec(f"eigvec.{k + 1}")
+        assert abs(np.linalg.norm(vk) - 1.0) < 1e-10
+        assert np.linalg.norm(Hd @ vk - ek * vk) < 1e-9
+
+
+def test_ed_solver1_converges_on_a_check_step(cuda, dense_small):
+    """The same solver on a spectrum without degeneracy: it stops on a check step (every 10
+    steps, src/lanczos.f90:89-110) with the oracle's eigenvalues and step count."""
+    import torch
+    from edrixs_b200 import device, solvers
+    g = dense_small
+    csr = orc.build_csr("ham_i", g["fock_i"], (g["hop_i_idx"], g["hop_i_val"]),
+                        (g["coul_i_idx"], g["coul_i_val"]), num_val_orbs=int(g["nv"]))
+    H = device.build_csr(device.HAM_I, device.basis_from_states(g["fock_i"]), (g["hop_i_idx"], g["hop_i_val"]),
+                         (g["coul_i_idx"], g["coul_i_val"]), num_val_orbs=int(g["nv"]))
+    e_o, v_o, nk_o = orc.lanczos_eigs(csr, 3, 500, 1e-8, nvec=2, seed=0)
+    e, v = solvers.plain_lanczos_eigs(H, 3, 2, 500, 1e-8, seed=0)
+    assert np.abs(e - e_o).max() < 1e-10
+    vh = v.cpu().numpy()
+    for j in range(2):  # the same vectors up to rounding (same start vector, same recurrence)
+        assert np.linalg.norm(vh[:, j] - v_o[:, j]) < 1e-8
+    torch.cuda.synchronize()
+
+
 def test_ed_thick_restart_lanczos(cuda, workdir):
     """ed_solver = 2 (ARPACK in the reference) -> block thick-restart Lanczos, 12870 states."""
     from edrixs_b200 import fedrixs, io, siam

@@ -85,12 +85,14 @@ class Resident:
         self.edge = None
         self.ops = {}
         self.packed = {}             # "hi" / "hn" -> device.PackedMatrix (None: too many values)
+        self.kron = {}               # "hi" / "hn" -> device.KronMatrix (None: no impurity x bath form)
         self.busy = 0
         self.last_used = time.monotonic()
 
     def nbytes(self):
         b = 0
-        for M in [self.Hi, self.Hn] + list(self.ops.values()) + list(self.packed.values()):
+        for M in [self.Hi, self.Hn] + list(self.ops.values()) + list(self.packed.values()) + \
+                list(self.kron.values()):
             if M is not None:
                 b += M.nbytes()
         if self.gs_v is not None:
@@ -113,6 +115,8 @@ class Resident:
                 self.Hi = device.build_csr(device.HAM_I, self.bi, self.terms["hop_i"], self.terms["coul_i"],
                                            num_val_orbs=s.nv)
                 self.packed["hi"] = device.pack(self.Hi)
+                self.kron["hi"] = device.kron_form(device.HAM_I, self.bi, self.terms["hop_i"], self.terms["coul_i"],
+                                                   num_val_orbs=s.nv)
             if self.gs_v is None or self.gs_v.shape[1] < ngs:
                 e, v = solvers.lowest_eigs(self.Hi, ngs, ngs, tol=1e-9, packed=self.packed.get("hi"))
                 self.gs_e, self.gs_v = np.asarray(e), v.contiguous()
@@ -121,6 +125,8 @@ class Resident:
                 self.Hn = device.build_csr(device.HAM_N, self.bn, self.terms["hop_n"], self.terms["coul_n"],
                                            num_val_orbs=s.nv, num_core_orbs=6)
                 self.packed["hn"] = device.pack(self.Hn)
+                self.kron["hn"] = device.kron_form(device.HAM_N, self.bn, self.terms["hop_n"], self.terms["coul_n"],
+                                                   num_val_orbs=s.nv, num_core_orbs=6)
                 e_n, _ = solvers.lowest_eigs(self.Hn, 1, 1, tol=1e-6, packed=self.packed.get("hn"))
                 self.edge = float(e_n[0] - self.gs_e[0])
             # the resident is shared with other workers' streams: finish building it here
@@ -361,7 +367,9 @@ class Server:
                              Dout=[res.op("out", p) for p in pouts], gs_e=gs_e[:G],
                              gs_v=gs_v[:, :G].contiguous(),
                              packed={k: v for k, v in (("hf", res.packed.get("hi")), ("hn", res.packed.get("hn")))
-                                     if v is not None})
+                                     if v is not None},
+                             kron={k: v for k, v in (("hf", res.kron.get("hi")), ("hn", res.kron.get("hn")))
+                                   if v is not None})
         out = rixs.rixs_spectra(P, allw, req.gamma_c, req.eloss, req.gamma_f, nkryl=req.nkryl,
                                 linsys_tol=req.linsys_tol, linsys_max=req.linsys_max, temperature=req.temperature,
                                 per_gs=True)
@@ -386,8 +394,11 @@ class Server:
             spans.append((c0, c0 + r.ngs))
             c0 += r.ngs
         phi = torch.cat(phis, dim=1).contiguous()
-        pk = res.packed.get("hn")
-        kr = device.krylov(res.Hn, phi, group[0][0].nkryl, apply=dict(packed=pk) if pk is not None else None)
+        kn, pk = res.kron.get("hn"), res.packed.get("hn")
+        if kn is not None:  # the slab product, on start vectors in its row order
+            kr = device.krylov(kn, kn.to_slab(phi), group[0][0].nkryl)
+        else:
+            kr = device.krylov(res.Hn, phi, group[0][0].nkryl, apply=dict(packed=pk) if pk is not None else None)
         norm = kr.norm.cpu().numpy()
         out = []
         for (r, _), (a, b) in zip(group, spans):

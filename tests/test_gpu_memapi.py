@@ -84,7 +84,16 @@ def test_rixs_in_memory_equals_the_files(cuda, golden_dir, workdir):
     src = os.path.join(golden_dir, "siam_callers")
     S, e, dm, noccu = _session(src)
     d = _drop_in(src, workdir, "rixs")
+    # both paths solve the shifted systems to 1e-13: the file path with one-RHS MINRES per
+    # point, the in-memory path with the batched shifted recurrences.  At the recorded 1e-10
+    # the two solutions differ by ~1e-10, which the 50-step final-state Lanczos at
+    # Gamma_f = 0.1 amplifies to ~3e-6 in the spectrum (the conditioning of the reference's
+    # own algorithm, not a difference of the paths).
+    txt = open("config.in").read().replace("linsys_tol=1e-10", "linsys_tol=1e-13").replace("linsys_max=500",
+                                                                                           "linsys_max=3000")
+    open("config.in", "w").write(txt)
     cfg = io.read_config("config.in")
+    assert cfg["linsys_tol"] == 1e-13
     fedrixs.rixs_fsolver(0, 0, 1)
     poles_f = io.read_poles(["rixs_poles.1"])
     eloss = np.linspace(-0.5, 12.0, 500)

@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--scale-omega", type=int, default=32)
     ap.add_argument("--scale-c64-omega", type=int, default=8,
                     help="incident energies (a subset of --scale-omega) of the complex64 RIXS comparison")
-    ap.add_argument("--kernel-case", choices=["apply", "hf-shapes", "all"], default=None,
+    ap.add_argument("--kernel-case", choices=["apply", "hf-shapes", "all", "kron"], default=None,
                     help="run only a small profiling case of the dominant kernels (for ncu)")
     return ap.parse_args()
 
@@ -98,6 +98,29 @@ def kernel_case(args):
     device.minres(Hn, b, 1e-300, 1, alpha=-1.0, sigma=40 + 0.6j)
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": "apply", "nnz_Hn": Hn.nnz, "nnz_Hf": Hf.nnz}))
+
+
+def kernel_case_kron(args):
+    """The slab product (k_lanczos_apply_kron) on this workload's matrices, for a profiler:
+    two Lanczos steps of H_f on 256 final-state columns (16 per block; the vectors, 0.76 GB,
+    exceed L2) and two of H_n on the 6 seed columns (its 97 MB of vectors fit in L2, as in the
+    timed step)."""
+    import torch
+    from edrixs_b200 import device
+    m, t = workload_terms(args.nbath, args.nelec)
+    nv, N = m.nv, args.nelec
+    bi, bn = device.fock_unrank(nv, N), device.fock_unrank(nv, N + 1)
+    Kf = device.kron_form(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
+    Kn = device.kron_form(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    W = torch.randn((Kf.nrows, 256), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    device.krylov(Kf, W, 2, apply=dict(col_group=16))
+    V = torch.randn((Kn.nrows, 6), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    device.krylov(Kn, V, 2)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": "kron", "rows_Hf": Kf.nrows, "rows_Hn": Kn.nrows, "slabs_Hf": Kf.spec.nslab,
+                      "slabs_Hn": Kn.spec.nslab}))
 
 
 def kernel_case_hf_shapes(args):
@@ -1134,6 +1157,8 @@ if __name__ == "__main__":
         kernel_case_hf_shapes(a)
     elif a.kernel_case == "all":
         kernel_case_all(a)
+    elif a.kernel_case == "kron":
+        kernel_case_kron(a)
     elif a.kernel_case:
         kernel_case(a)
     elif a.impl == "reference":

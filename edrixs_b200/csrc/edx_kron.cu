@@ -27,6 +27,7 @@
 namespace edx {
 
 constexpr int KR_NT = 256;       // threads per block
+constexpr int KR_CW = 8;         // columns per column tile: one 128-byte line per staged row
 constexpr int KR_BOXR = 32;      // rows per tensor-load box
 constexpr int KR_NBUF = 3;       // source slabs staged ahead
 constexpr uint32_t KR_WAIT_LIMIT = 1u << 21;
@@ -124,35 +125,35 @@ __device__ __forceinline__ int sig_ann(uint32_t cfg, int m, int a, int n_alo) {
 }
 
 // ---- the slab product ---------------------------------------------------------------------
-// grid (gx, column tiles); block b owns slabs b, b + gx, ...; thread (g, c) owns rows
-// g, g + G, ... (RPT of them) of each slab in column c0 + c.  LANCZOS: the fused step of
-// k_lanczos_apply_packed (W = scur (H U_i) - beta_{i-1} sprev U_{i-1} into Y = V_prev, alpha
-// partials, the last block of each column tile finishes alpha in block order); otherwise
-// Y = H X.
-template <int CW, int RPT, bool LANCZOS>
+// grid (gx, column tiles of KR_CW); block b owns slabs b, b + gx, ...; thread t owns rows
+// t, t + KR_NT, ... (RPT of them) of each slab and all KC columns of the tile, so the
+// per-hop work (neighbour rank, sign, coefficient) is paid once for KC columns.  A staged
+// slab is rows of 8 complex values (128 bytes) laid out by the tensor unit's 128-byte
+// swizzle: value (r, c) sits at r * 8 + (c ^ (r & 7)), so lanes reading different rows spread
+// over the banks.  LANCZOS: the fused step of k_lanczos_apply_packed (W = scur (H U_i) -
+// beta_{i-1} sprev U_{i-1} into Y = V_prev, alpha partials, the last block of each column
+// tile finishes alpha in block order); otherwise Y = H X.
+template <int KC, int RPT, bool LANCZOS>
 __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const __grid_constant__ CUtensorMap tm,
                                                               const double2* __restrict__ X, double2* __restrict__ Y,
                                                               KrylovState S, int k, int it, int stage_rows,
                                                               unsigned* __restrict__ tile_ticket,
                                                               int* __restrict__ err) {
-    constexpr int G = KR_NT / CW;
-    extern __shared__ __align__(128) unsigned char kr_smem[];
-    // tensor-load destinations must start on a 128-byte boundary: align the ring explicitly
-    // (the host asks for 128 spare bytes)
-    double2* stages = reinterpret_cast<double2*>(kr_smem + ((128u - (smem_addr(kr_smem) & 127u)) & 127u));
-    const int stage_elems = stage_rows * CW;
+    constexpr int NW = KR_NT / 32;
+    extern __shared__ __align__(1024) unsigned char kr_smem[];
+    // swizzled tensor-load destinations start on a 1024-byte boundary: align explicitly (the
+    // host asks for 1024 spare bytes)
+    double2* stages = reinterpret_cast<double2*>(kr_smem + ((1024u - (smem_addr(kr_smem) & 1023u)) & 1023u));
+    const int stage_elems = stage_rows * KR_CW;
     double2* tcre = stages + KR_NBUF * stage_elems;
     double2* tann = tcre + K.nah * K.nb;
     uint64_t* bar = reinterpret_cast<uint64_t*>(tann + K.nah * K.nb);
-    __shared__ double red[KR_NT];
+    __shared__ double wred[NW][KC];
     __shared__ bool sh_last;
 
-    const int tid = threadIdx.x;
-    const int g = tid / CW, c = tid % CW;
-    const bool act = g < G;
-    const int c0 = blockIdx.y * CW;
-    const int gcol = c0 + c;
-    const bool colok = act && gcol < k;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int c0 = blockIdx.y * KR_CW;
+    const int kc = min(KC, k - c0);  // columns of this tile that exist
 
     for (int i = tid; i < K.nah * K.nb; i += KR_NT) {
         tcre[i] = K.t_cre[i];
@@ -190,9 +191,9 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         const int nbox = (rows + KR_BOXR - 1) / KR_BOXR;
         const int st = (int)(issued % KR_NBUF);
         double2* dst = stages + st * stage_elems;
-        mbar_expect_tx(&bar[st], (unsigned)(nbox * KR_BOXR * CW * (int)sizeof(double2)));
+        mbar_expect_tx(&bar[st], (unsigned)(nbox * KR_BOXR * KR_CW * (int)sizeof(double2)));
         for (int bx = 0; bx < nbox; ++bx)
-            tma_load_2d(dst + bx * KR_BOXR * CW, &tm, 2 * c0, r0 + bx * KR_BOXR, &bar[st]);
+            tma_load_2d(dst + bx * KR_BOXR * KR_CW, &tm, 2 * c0, r0 + bx * KR_BOXR, &bar[st]);
         ++issued;
         return true;
     };
@@ -200,12 +201,16 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         for (int i = 0; i < KR_NBUF; ++i)
             if (!issue_next()) break;
 
-    double bprev = 0.0, scur = 0.0;
-    if (LANCZOS && colok) {
-        bprev = it > 0 ? S.beta[gcol] * S.sprev[gcol] : 0.0;
-        scur = S.scur[gcol];
+    double bprev[KC], scur[KC], apart[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+        bprev[j] = scur[j] = apart[j] = 0.0;
+        if (LANCZOS && j < kc) {
+            bprev[j] = it > 0 ? S.beta[c0 + j] * S.sprev[c0 + j] : 0.0;
+            scur[j] = S.scur[c0 + j];
+        }
     }
-    double apart = 0.0;
+    const uint32_t full = (1u << K.nb) - 1u;
     unsigned consumed = 0;
     bool bad = false;
     for (int s = blockIdx.x; s < K.nslab && !bad; s += gridDim.x) {
@@ -215,22 +220,28 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         const uint32_t cfg = K.slab_cfg[s];
         const int bo = K.b_off[m];
         const int64_t sb = K.src_ptr[s], se = K.src_ptr[s + 1];
-        double2 acc[RPT];
+        double2 acc[RPT][KC];
+        uint32_t Bv[RPT];
 #pragma unroll
-        for (int j = 0; j < RPT; ++j) acc[j] = make_double2(0.0, 0.0);
+        for (int q = 0; q < RPT; ++q) {
+            const int r = tid + q * KR_NT;
+            Bv[q] = r < R ? __ldg(K.b_cfg + bo + r) : 0u;
+#pragma unroll
+            for (int j = 0; j < KC; ++j) acc[q][j] = make_double2(0.0, 0.0);
+        }
         for (int64_t js = sb; js < se; ++js) {
             const int st = (int)(consumed % KR_NBUF);
             const unsigned par = (consumed / KR_NBUF) & 1u;
             const bool ok = mbar_wait_bounded(&bar[st], par);
-            if (ok && act) {
+            if (ok) {
                 const double2* Xs = stages + st * stage_elems;
                 const int kind = K.src_kind[js];
                 const int type = kind & 15, q = kind >> 4;
                 if (type <= EDX_KRON_SRC_OWN) {
                     const double2 v0 = K.src_coef[js];
 #pragma unroll
-                    for (int j = 0; j < RPT; ++j) {
-                        const int r = g + G * j;
+                    for (int qq = 0; qq < RPT; ++qq) {
+                        const int r = tid + qq * KR_NT;
                         if (r < R) {
                             double2 v = v0;
                             if (type == EDX_KRON_SRC_OWN) {
@@ -238,7 +249,9 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
                                 v.x += d.x;
                                 v.y += d.y;
                             }
-                            acc[j] = fma_c(v, Xs[r * CW + c], acc[j]);
+                            const double2* xr = Xs + r * KR_CW;
+#pragma unroll
+                            for (int j = 0; j < KC; ++j) acc[qq][j] = fma_c(v, xr[j ^ (r & 7)], acc[qq][j]);
                         }
                     }
                 } else {
@@ -246,12 +259,11 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
                     const int a = K.hyb_a[q];
                     const int sa = cre ? sig_cre(cfg, m, a, K.n_alo) : sig_ann(cfg, m, a, K.n_alo);
                     const double2* T = (cre ? tcre : tann) + q * K.nb;
-                    const uint32_t full = (1u << K.nb) - 1u;
 #pragma unroll
-                    for (int j = 0; j < RPT; ++j) {
-                        const int r = g + G * j;
+                    for (int qq = 0; qq < RPT; ++qq) {
+                        const int r = tid + qq * KR_NT;
                         if (r < R) {
-                            const uint32_t B = __ldg(K.b_cfg + bo + r);
+                            const uint32_t B = Bv[qq];
                             const uint16_t* nbr = K.b_nbr + (size_t)(bo + r) * K.nb;
                             uint32_t bits = cre ? B : (~B & full);
                             while (bits) {
@@ -263,7 +275,9 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
                                     t.x = -t.x;
                                     t.y = -t.y;
                                 }
-                                acc[j] = fma_c(t, Xs[rs * CW + c], acc[j]);
+                                const double2* xr = Xs + rs * KR_CW;
+#pragma unroll
+                                for (int j = 0; j < KC; ++j) acc[qq][j] = fma_c(t, xr[j ^ (rs & 7)], acc[qq][j]);
                             }
                         }
                     }
@@ -279,22 +293,25 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
             }
         }
         if (bad) break;
-        if (colok) {
 #pragma unroll
-            for (int j = 0; j < RPT; ++j) {
-                const int r = g + G * j;
-                if (r < R) {
-                    const int64_t o = (int64_t)(off + r) * k + gcol;
-                    if (LANCZOS) {
-                        const double2 vc = X[o];
-                        const double2 vp = Y[o];
-                        double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
-                        w.x = w.x + scur * acc[j].x;
-                        w.y = w.y + scur * acc[j].y;
-                        Y[o] = w;
-                        apart += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
-                    } else {
-                        Y[o] = acc[j];
+        for (int qq = 0; qq < RPT; ++qq) {
+            const int r = tid + qq * KR_NT;
+            if (r < R) {
+                const int64_t o = (int64_t)(off + r) * k + c0;
+#pragma unroll
+                for (int j = 0; j < KC; ++j) {
+                    if (j < kc) {
+                        if (LANCZOS) {
+                            const double2 vc = X[o + j];
+                            const double2 vp = Y[o + j];
+                            double2 w = make_double2(-bprev[j] * vp.x, -bprev[j] * vp.y);
+                            w.x = w.x + scur[j] * acc[qq][j].x;
+                            w.y = w.y + scur[j] * acc[qq][j].y;
+                            Y[o + j] = w;
+                            apart[j] += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
+                        } else {
+                            Y[o + j] = acc[qq][j];
+                        }
                     }
                 }
             }
@@ -309,12 +326,18 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         return;
     }
     if (!LANCZOS) return;
-    // alpha partials of this block, then the last block of the column tile adds them in block order
-    red[tid] = colok ? apart : 0.0;
+    // alpha partials: a fixed butterfly inside each warp, then the warps in order
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+        double v = apart[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) wred[warp][j] = v;
+    }
     __syncthreads();
-    if (tid < CW && c0 + tid < k) {
+    if (tid < kc) {
         double t = 0.0;
-        for (int gg = 0; gg < G; ++gg) t += red[gg * CW + tid];
+        for (int w = 0; w < NW; ++w) t += wred[w][tid];
         S.part[(int64_t)blockIdx.x * k + c0 + tid] = t;
     }
     __threadfence();
@@ -323,7 +346,8 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
     __syncthreads();
     if (!sh_last) return;
     __threadfence();
-    for (int j = 0; j < CW && c0 + j < k; ++j) {
+    __shared__ double red[KR_NT];
+    for (int j = 0; j < kc; ++j) {
         const int col = c0 + j;
         double t = 0.0;
         for (int b = tid; b < (int)gridDim.x; b += KR_NT) t += __ldcg(S.part + (int64_t)b * k + col);
@@ -357,28 +381,23 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
     return fn;
 }
 
-static bool cw_supported(int cw) {
-    return cw == 1 || cw == 2 || cw == 4 || cw == 6 || cw == 8 || cw == 12 || cw == 16;
-}
-
-static int default_cw(int k) {
-    const int ws[] = {1, 2, 4, 6, 8, 12, 16};
-    for (int w : ws)
+// columns computed per thread: the smallest supported count >= k within the 8-column tile
+static int kc_of(int k) {
+    for (int w : {1, 2, 4, 6, 8})
         if (w >= k) return w;
-    return 16;
+    return 8;
 }
 
 static int stage_rows_of(const edx_kron* K) { return (K->max_rows + KR_BOXR - 1) / KR_BOXR * KR_BOXR; }
 
-static size_t smem_bytes(const edx_kron* K, int cw) {
-    return 128 + (size_t)KR_NBUF * stage_rows_of(K) * cw * sizeof(double2) +
+static size_t smem_bytes(const edx_kron* K) {
+    return 1024 + (size_t)KR_NBUF * stage_rows_of(K) * KR_CW * sizeof(double2) +
            2 * (size_t)K->nah * K->nb * sizeof(double2) + KR_NBUF * sizeof(uint64_t);
 }
 
-static int rpt_of(const edx_kron* K, int cw) {
-    const int G = KR_NT / cw;
-    for (int r : {4, 8, 16})
-        if (r * G >= K->max_rows) return r;
+static int rpt_of(const edx_kron* K) {
+    for (int r : {1, 2, 4})
+        if (r * KR_NT >= K->max_rows) return r;
     return 0;
 }
 
@@ -395,79 +414,77 @@ int kron_check(const edx_kron* K) {
     return EDX_OK;
 }
 
-int kron_grid_x(const edx_kron* K, int k, int cw) {
-    const size_t sm = smem_bytes(K, cw);
+int kron_grid_x(const edx_kron* K, int k, int /*col_group*/) {
+    const size_t sm = smem_bytes(K);
     int occ = (int)std::min<size_t>(8, (size_t)(227 * 1024) / std::max<size_t>(sm + 2048, 1));
     if (occ < 1) occ = 1;
-    const int ntile = (k + cw - 1) / cw;
+    const int ntile = (k + KR_CW - 1) / KR_CW;
     const int64_t target = (int64_t)num_sms() * occ * 4;
     int64_t gx = (target + ntile - 1) / ntile;
     gx = std::max<int64_t>(1, std::min<int64_t>(gx, K->nslab));
     return (int)gx;
 }
 
-int kron_tensor_map(const edx_kron* K, const double2* X, int k, int cw, void* out) {
+// 2-D tensor map of an n x k complex128 block (row-major) as doubles, boxes of 32 rows x 8
+// complex values, 128-byte swizzle.  Columns past k (k < 8, or the last tile) read as zeros.
+int kron_tensor_map(const edx_kron* K, const double2* X, int k, int /*col_group*/, void* out) {
     auto fn = encode_tiled();
     if (!fn) return fail(EDX_ERR_CUDA, "slab form: cuTensorMapEncodeTiled is not available from the driver");
     cuuint64_t dims[2] = {(cuuint64_t)2 * k, (cuuint64_t)K->nrows};
     cuuint64_t strides[1] = {(cuuint64_t)2 * k * sizeof(double)};
-    cuuint32_t box[2] = {(cuuint32_t)(2 * cw), (cuuint32_t)KR_BOXR};
+    cuuint32_t box[2] = {(cuuint32_t)(2 * KR_CW), (cuuint32_t)KR_BOXR};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(reinterpret_cast<CUtensorMap*>(out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double2*>(X),
-                    dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(EDX_ERR_CUDA, "slab form: cuTensorMapEncodeTiled failed (%d)", (int)r);
     return EDX_OK;
 }
 
-template <int CW, int RPT, bool LANCZOS>
+template <int KC, int RPT, bool LANCZOS>
 static int launch_kron_rpt(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
                            int k, int it, unsigned* tt, int* err, cudaStream_t st) {
-    auto kern = k_lanczos_apply_kron<CW, RPT, LANCZOS>;
-    const size_t sm = smem_bytes(K, CW);
-    EDX_REQUIRE(sm <= 227 * 1024, "slab form: %zu bytes of staged slabs exceed shared memory (use fewer columns)",
-                sm);
+    auto kern = k_lanczos_apply_kron<KC, RPT, LANCZOS>;
+    const size_t sm = smem_bytes(K);
+    EDX_REQUIRE(sm <= 227 * 1024, "slab form: %zu bytes of staged slabs exceed shared memory", sm);
     EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int ntile = (k + CW - 1) / CW;
+    const int ntile = (k + KR_CW - 1) / KR_CW;
     EDX_REQUIRE(ntile <= 65535, "slab form: too many column tiles");
-    dim3 grid(kron_grid_x(K, k, CW), ntile);
+    dim3 grid(kron_grid_x(K, k, 0), ntile);
     kern<<<grid, KR_NT, sm, st>>>(view_of(K), *tm, X, Y, S, k, it, stage_rows_of(K), tt, err);
     EDX_CHECK_LAUNCH();
     return EDX_OK;
 }
 
-template <int CW, bool LANCZOS>
-static int launch_kron_cw(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
+template <int KC, bool LANCZOS>
+static int launch_kron_kc(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
                           int k, int it, unsigned* tt, int* err, cudaStream_t st) {
-    switch (rpt_of(K, CW)) {
-    case 4: return launch_kron_rpt<CW, 4, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
-    case 8: return launch_kron_rpt<CW, 8, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
-    case 16: return launch_kron_rpt<CW, 16, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    switch (rpt_of(K)) {
+    case 1: return launch_kron_rpt<KC, 1, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 2: return launch_kron_rpt<KC, 2, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 4: return launch_kron_rpt<KC, 4, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
     }
-    return fail(EDX_ERR_INVALID, "slab form: slabs of %d rows are too long for %d columns per block", K->max_rows, CW);
+    return fail(EDX_ERR_INVALID, "slab form: slabs of %d rows exceed the %d rows a block holds", K->max_rows,
+                4 * KR_NT);
 }
 
 template <bool LANCZOS>
 static int launch_kron(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
-                       int k, int it, unsigned* tt, int* err, int cw, cudaStream_t st) {
-    switch (cw) {
-    case 1: return launch_kron_cw<1, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
-    case 2: return launch_kron_cw<2, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
-    case 4: return launch_kron_cw<4, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
-    case 6: return launch_kron_cw<6, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
-    case 8: return launch_kron_cw<8, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
-    case 12: return launch_kron_cw<12, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
-    case 16: return launch_kron_cw<16, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+                       int k, int it, unsigned* tt, int* err, cudaStream_t st) {
+    switch (kc_of(k)) {
+    case 1: return launch_kron_kc<1, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 2: return launch_kron_kc<2, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 4: return launch_kron_kc<4, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    case 6: return launch_kron_kc<6, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
+    default: return launch_kron_kc<8, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
     }
-    return fail(EDX_ERR_INVALID, "slab form: columns per block must be 1, 2, 4, 6, 8, 12 or 16 (got %d)", cw);
 }
 
-int kron_col_group(int k, int requested) { return requested > 0 ? requested : default_cw(k); }
+int kron_col_group(int /*k*/, int /*requested*/) { return KR_CW; }
 
 int apply_kron(const edx_kron* K, const void* tmap, const double2* Vc, double2* Vp, const KrylovState& S, int it,
                unsigned* tile_ticket, int* err, int col_group, cudaStream_t st) {
-    return launch_kron<true>(K, static_cast<const CUtensorMap*>(tmap), Vc, Vp, S, S.k, it, tile_ticket, err,
-                             col_group, st);
+    return launch_kron<true>(K, static_cast<const CUtensorMap*>(tmap), Vc, Vp, S, S.k, it, tile_ticket, err, st);
 }
 
 __global__ void k_permute_rows(int64_t n, int k, const double2* __restrict__ src, int64_t lds,
@@ -495,8 +512,8 @@ extern "C" int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double
     int rc = kron_check(K);
     if (rc) return rc;
     EDX_REQUIRE(k >= 1 && d_x && d_y && d_x != d_y, "edx_kron_spmm: bad arguments");
-    const int cw = kron_col_group(k, col_group);
-    EDX_REQUIRE(cw_supported(cw), "edx_kron_spmm: col_group must be 1, 2, 4, 6, 8, 12 or 16");
+    (void)col_group;  // the slab product always works on 8-column tiles
+    const int cw = KR_CW;
     Workspace w(d_work, work_bytes);
     int* err = w.take<int>(1);
     if (!err) return fail(EDX_ERR_WORKSPACE, "edx_kron_spmm: workspace too small");
@@ -506,7 +523,7 @@ extern "C" int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double
     if ((rc = kron_tensor_map(K, reinterpret_cast<const double2*>(d_x), k, cw, &tm))) return rc;
     KrylovState S{};
     rc = launch_kron<false>(K, &tm, reinterpret_cast<const double2*>(d_x), reinterpret_cast<double2*>(d_y), S, k, 0,
-                            nullptr, err, cw, st);
+                            nullptr, err, st);
     if (rc) return rc;
     int h = 0;
     EDX_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -37,11 +37,9 @@ def candidates(k):
 
 
 def kron_candidates(k):
-    """Columns per block of the slab product worth timing for k columns."""
-    if k > 16:
-        return [16, 8]
-    first = next(w for w in (1, 2, 4, 6, 8, 12, 16) if w >= k)
-    return sorted({first, min(16, 2 * first) if first < 16 else 16})
+    """Launch shapes of the slab product worth timing for k columns (it always works on
+    8-column tiles, so there is one)."""
+    return [8]
 
 
 def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, packed=None, kron=None):

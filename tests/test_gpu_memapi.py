@@ -104,7 +104,13 @@ def test_rixs_in_memory_equals_the_files(cuda, golden_dir, workdir):
                          nkryl=cfg["nkryl"], linsys_max=cfg["linsys_max"], linsys_tol=cfg["linsys_tol"],
                          temperature=1.0)
     assert rixs.shape == (1, 500, 1)
-    assert np.abs(rixs[0, :, 0] - spec_f).max() <= 1e-6 * np.abs(spec_f).max()
     p = poles[0][0]
+    # the pole file writes the normalisation |D_out^+ x|^2 with 10 decimals (f20.10,
+    # src/io.f90:532-537); for this start vector that is ~1e-5 relative.  Compare it to the
+    # file's last decimal, and the spectra with their normalisation divided out.
+    nm, nf = p["norm"][0], poles_f["norm"][0]
+    assert abs(nm - nf) <= 6e-11
+    shape_m, shape_f = rixs[0, :, 0] / nm, spec_f / nf
+    assert np.abs(shape_m - shape_f).max() <= 1e-6 * np.abs(shape_f).max()
     assert p["npoles"] == poles_f["npoles"]
     assert np.abs(np.array(p["alpha"][0]) - np.array(poles_f["alpha"][0])).max() < 1e-8

@@ -101,26 +101,37 @@ def kernel_case(args):
 
 
 def kernel_case_kron(args):
-    """The slab product (k_lanczos_apply_kron) on this workload's matrices, for a profiler:
-    two Lanczos steps of H_f on 256 final-state columns (16 per block; the vectors, 0.76 GB,
-    exceed L2) and two of H_n on the 6 seed columns (its 97 MB of vectors fit in L2, as in the
-    timed step)."""
+    """The apply kernels of this workload side by side, for a profiler: the packed product on
+    H_f (256 final-state columns at the autotuner's usual shape; the vectors, 0.76 GB, exceed
+    L2), and on H_n (6 seed columns, one row per lane group) next to the slab product on H_n.
+    Every product runs one warm-up step first, then one step each in the order packed H_f,
+    slab H_n, packed H_n (launches 4-6 of k_lanczos_apply*)."""
     import torch
     from edrixs_b200 import device
     m, t = workload_terms(args.nbath, args.nelec)
     nv, N = m.nv, args.nelec
     bi, bn = device.fock_unrank(nv, N), device.fock_unrank(nv, N + 1)
-    Kf = device.kron_form(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
+    Hf = device.build_csr(device.HAM_I, bi, t["hop_i"], t["coul_i"], num_val_orbs=nv)
+    Hn = device.build_csr(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    Pf, Pn = device.pack(Hf), device.pack(Hn)
     Kn = device.kron_form(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    nnz_f, nnz_n = Hf.nnz, Hn.nnz
+    del Hf, Hn  # only the packed and slab forms stay on the device (about 3 GB in all)
+    torch.cuda.empty_cache()
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
-    W = torch.randn((Kf.nrows, 256), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
-    device.krylov(Kf, W, 2, apply=dict(col_group=16))
-    V = torch.randn((Kn.nrows, 6), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
-    device.krylov(Kn, V, 2)
-    torch.cuda.synchronize()
-    print(json.dumps({"kernel_case": "kron", "rows_Hf": Kf.nrows, "rows_Hn": Kn.nrows, "slabs_Hf": Kf.spec.nslab,
-                      "slabs_Hn": Kn.spec.nslab}))
+    W = torch.randn((Pf.nrows, 256), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    V = torch.randn((Pn.nrows, 6), dtype=torch.float64, device="cuda", generator=g).to(torch.complex128)
+    Vs = Kn.to_slab(V)
+    hf = dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1, chunked=0)
+    hn = dict(col_group=6, threads=1024, blocks_per_sm=1, rowslot=1)
+    runs = [(Pf, W, hf), (Kn, Vs, None), (Pn, V, hn)]
+    for _ in range(2):  # a warm-up step of each, then the profiled one
+        for A, X, ap in runs:
+            device.krylov(A, X, 1, apply=ap)
+        torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": "kron", "rows_Hf": Pf.nrows, "rows_Hn": Pn.nrows, "slabs_Hn": Kn.spec.nslab,
+                      "nnz_Hf": nnz_f, "nnz_Hn": nnz_n}))
 
 
 def kernel_case_hf_shapes(args):

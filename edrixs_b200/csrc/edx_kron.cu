@@ -94,16 +94,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
     return ok != 0;
 }
 // true once the phase with this parity has completed; false after KR_WAIT_LIMIT rounds
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, unsigned parity) {
-    if (mbar_try_wait(b, parity)) return true;
+__device__ __noinline__ bool mbar_wait_bounded(uint64_t* b, unsigned parity) {
     for (uint32_t i = 0; i < KR_WAIT_LIMIT; ++i) {
         if (mbar_try_wait(b, parity)) return true;
-        if (i >= 64) __nanosleep(64);
+        if (i >= 8) __nanosleep(128);
     }
     return false;
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
 }
 // 2-D tiled tensor load of one box into shared memory; completion counted on `bar`.  The
 // innermost coordinate x is a multiple of 2 doubles (16 bytes) by construction.
@@ -151,8 +147,7 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
     const int stage_elems = stage_rows * KR_CW;
     double2* tcre = stages + KR_NBUF * stage_elems;
     double2* tann = tcre + K.nah * K.nb;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(tann + K.nah * K.nb);  // stage filled (tensor loads)
-    uint64_t* emp = bar + KR_NBUF;                                       // stage drained (every thread)
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tann + K.nah * K.nb);
     __shared__ double wred[NW][KC];
     __shared__ bool sh_last;
 
@@ -165,18 +160,13 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         tann[i] = K.t_ann[i];
     }
     if (tid == 0) {
-        for (int b = 0; b < KR_NBUF; ++b) {
-            mbar_init(&bar[b], 1);
-            mbar_init(&emp[b], KR_NT);
-        }
+        for (int b = 0; b < KR_NBUF; ++b) mbar_init(&bar[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
     // producer cursor (thread 0): the next source to stage is source p_beg + p_j of slab
-    // p_slab (every slab has at least its own slab as a source).  A stage is refilled only
-    // once every thread has drained it (emp), so the other warps run up to KR_NBUF sources
-    // ahead instead of meeting at a block barrier per source.
+    // p_slab (every slab has at least its own slab as a source)
     int p_slab = blockIdx.x, p_j = 0;
     int64_t p_beg = 0, p_end = 0;
     if (p_slab < K.nslab) {
@@ -184,8 +174,7 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         p_end = K.src_ptr[p_slab + 1];
     }
     unsigned issued = 0;
-    // 1: staged the next source; 0: none left; -1: a drain did not complete in time
-    auto issue_next = [&]() -> int {
+    auto issue_next = [&]() -> bool {
         while (p_slab < K.nslab && p_beg + p_j >= p_end) {
             p_slab += gridDim.x;
             p_j = 0;
@@ -194,31 +183,33 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
                 p_end = K.src_ptr[p_slab + 1];
             }
         }
-        if (p_slab >= K.nslab) return 0;
-        const int st = (int)(issued % KR_NBUF);
-        if (issued >= (unsigned)KR_NBUF) {  // wait until every thread has drained this stage
-            if (!mbar_wait_bounded(&emp[st], ((issued / KR_NBUF) - 1u) & 1u)) return -1;
-            fence_proxy_async();
-        }
+        if (p_slab >= K.nslab) return false;
         const int sl = K.src_slab[p_beg + p_j];
         ++p_j;
         const int r0 = K.slab_off[sl];
         const int rows = K.slab_off[sl + 1] - r0;
         const int nbox = (rows + KR_BOXR - 1) / KR_BOXR;
+        const int st = (int)(issued % KR_NBUF);
         double2* dst = stages + st * stage_elems;
         mbar_expect_tx(&bar[st], (unsigned)(nbox * KR_BOXR * KR_CW * (int)sizeof(double2)));
         for (int bx = 0; bx < nbox; ++bx)
             tma_load_2d(dst + bx * KR_BOXR * KR_CW, &tm, 2 * c0, r0 + bx * KR_BOXR, &bar[st]);
         ++issued;
-        return 1;
+        return true;
     };
     if (tid == 0)
         for (int i = 0; i < KR_NBUF; ++i)
-            if (issue_next() <= 0) break;
+            if (!issue_next()) break;
 
-    double apart[KC];
+    double bprev[KC], scur[KC], apart[KC];
 #pragma unroll
-    for (int j = 0; j < KC; ++j) apart[j] = 0.0;
+    for (int j = 0; j < KC; ++j) {
+        bprev[j] = scur[j] = apart[j] = 0.0;
+        if (LANCZOS && j < kc) {
+            bprev[j] = it > 0 ? S.beta[c0 + j] * S.sprev[c0 + j] : 0.0;
+            scur[j] = S.scur[c0 + j];
+        }
+    }
     const uint32_t full = (1u << K.nb) - 1u;
     unsigned consumed = 0;
     bool bad = false;
@@ -241,8 +232,7 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         for (int64_t js = sb; js < se; ++js) {
             const int st = (int)(consumed % KR_NBUF);
             const unsigned par = (consumed / KR_NBUF) & 1u;
-            const bool ok = !bad && mbar_wait_bounded(&bar[st], par);
-            bad = !ok;
+            const bool ok = mbar_wait_bounded(&bar[st], par);
             if (ok) {
                 const double2* Xs = stages + st * stage_elems;
                 const int kind = K.src_kind[js];
@@ -294,11 +284,15 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
                 }
             }
             ++consumed;
-            if (ok) mbar_arrive(&emp[st]);
-            // thread 0 stages the next source once this one is drained everywhere; a load or
-            // drain that does not arrive in time leaves `bad` set and stops the staging
-            if (tid == 0 && !bad && issued < consumed + KR_NBUF && issue_next() < 0) bad = true;
+            // every thread is done with this stage (and all agree whether a load was lost)
+            bad = __syncthreads_or(!ok) != 0;
+            if (bad) break;
+            if (tid == 0) {
+                fence_proxy_async();
+                issue_next();
+            }
         }
+        if (bad) break;
 #pragma unroll
         for (int qq = 0; qq < RPT; ++qq) {
             const int r = tid + qq * KR_NT;
@@ -308,14 +302,11 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
                 for (int j = 0; j < KC; ++j) {
                     if (j < kc) {
                         if (LANCZOS) {
-                            // the column's scalars are read here rather than held in registers
-                            const double bprev = it > 0 ? __ldg(S.beta + c0 + j) * __ldg(S.sprev + c0 + j) : 0.0;
-                            const double scur = __ldg(S.scur + c0 + j);
                             const double2 vc = X[o + j];
                             const double2 vp = Y[o + j];
-                            double2 w = make_double2(-bprev * vp.x, -bprev * vp.y);
-                            w.x = w.x + scur * acc[qq][j].x;
-                            w.y = w.y + scur * acc[qq][j].y;
+                            double2 w = make_double2(-bprev[j] * vp.x, -bprev[j] * vp.y);
+                            w.x = w.x + scur[j] * acc[qq][j].x;
+                            w.y = w.y + scur[j] * acc[qq][j].y;
                             Y[o + j] = w;
                             apart[j] += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
                         } else {
@@ -326,11 +317,11 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
             }
         }
     }
-    if (__syncthreads_or(bad)) {
+    if (bad) {
         if (tid == 0) {
             atomicExch(err, 1);
             // the loads still in flight land before the block's shared memory is released
-            for (unsigned u = consumed; u < issued; ++u) mbar_wait_bounded(&bar[u % KR_NBUF], (u / KR_NBUF) & 1u);
+            for (unsigned u = consumed - 1; u < issued; ++u) mbar_wait_bounded(&bar[u % KR_NBUF], (u / KR_NBUF) & 1u);
         }
         return;
     }
@@ -401,7 +392,7 @@ static int stage_rows_of(const edx_kron* K) { return (K->max_rows + KR_BOXR - 1)
 
 static size_t smem_bytes(const edx_kron* K) {
     return 1024 + (size_t)KR_NBUF * stage_rows_of(K) * KR_CW * sizeof(double2) +
-           2 * (size_t)K->nah * K->nb * sizeof(double2) + 2 * KR_NBUF * sizeof(uint64_t);
+           2 * (size_t)K->nah * K->nb * sizeof(double2) + KR_NBUF * sizeof(uint64_t);
 }
 
 static int rpt_of(const edx_kron* K) {

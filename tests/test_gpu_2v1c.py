@@ -38,7 +38,7 @@ def dense():
 
 def _stage(tmp_path, name, e0=None, g0=None):
     """A working directory with the ED files and those of one XAS / RIXS caller run."""
-    d = tmp_path / name
+    d = tmp_path / (name + "_run")
     d.mkdir()
     for src in (os.path.join(G, "ed_00"), os.path.join(G, name)):
         for fn in os.listdir(src):
@@ -69,14 +69,14 @@ def test_2v1c_ed_xas_rixs_on_the_gpu(cuda, dense, tmp_path, monkeypatch):
     edge = np.linalg.eigvalsh(dense["H_n"])[0] - e0
     om = edge + np.linspace(-3.0, 12.0, 301)
     for name in ("xas_01", "xas_02"):
-        monkeypatch.chdir(_stage(tmp_path, name + "_run", e0, g0))
+        monkeypatch.chdir(_stage(tmp_path, name, e0, g0))
         fedrixs.xas_fsolver(0, 0, 1)
         spec = orc.spectra_from_poles(edxio.read_poles(["xas_poles.1"]), om, 0.3, 1.0)
         exact = _kh(dense["H_n"], dense[f"D_{name}"] @ g0, e0, om, 0.3)
         assert np.abs(spec - exact).max() <= 1e-6 * np.abs(exact).max(), name
     eloss = np.linspace(-0.5, 6.0, 131)
     for name in ("rixs_03", "rixs_04"):
-        monkeypatch.chdir(_stage(tmp_path, name + "_run", e0, g0))
+        monkeypatch.chdir(_stage(tmp_path, name, e0, g0))
         cfg = edxio.read_config("config.in")
         fedrixs.rixs_fsolver(0, 0, 1)
         poles = edxio.read_poles(["rixs_poles.1"])

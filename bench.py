@@ -161,7 +161,8 @@ def kernel_case_all(args):
     forms with the packer, two MINRES steps on H_n, the continued fraction
     (768 pole sets x 2000 points), the density matrix, the packed SpMM (narrow and wide
     forms), the Gram-Schmidt and CholeskyQR passes of the eigensolver, the few-column Lanczos
-    products with one row per lane group, and 16 Lanczos steps with streamed projections."""
+    products with one row per lane group, 16 Lanczos steps with streamed projections, and the
+    slab form of H_n (product, Lanczos step, row permutations)."""
     import torch
     from edrixs_b200 import device
     m, t = workload_terms(args.nbath, args.nelec)
@@ -219,6 +220,12 @@ def kernel_case_all(args):
     acc = torch.zeros((Dout.nrows, 24), dtype=torch.complex128, device="cuda")
     device.krylov(Hn, seeds, 16, proj=[Dout], apply=dict(packed=Pn),
                   accumulate=dict(window=8, col=shifts[0], coef=coef, out=[acc]))
+    # the slab form of H_n: its product, a Lanczos step on it, and the row permutations
+    Kn = device.kron_form(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    Vs = Kn.to_slab(V)
+    device.spmm(Kn, Vs)
+    device.krylov(Kn, Vs, 2)
+    Kn.from_slab(Vs)
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": "all", "nnz_Hn": Hn.nnz, "nnz_Hf": Hf.nnz, "nnz_Din": Din.nnz,
                       "nnz_Dout": Dout.nnz}))

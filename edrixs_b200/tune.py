@@ -86,10 +86,12 @@ def tune_apply(A: device.CSR, k, c64=False, steps=3, verbose=False, packed=None,
     final = [(time_of(cfg, 2 * steps), cfg) for _, cfg in results[:4]]
     best_t, best = min(final, key=lambda x: x[0])
     # within 3% of the fastest, prefer the form that reads fewer matrix bytes (slab, then
-    # packed, then CSR): such near-ties flip with noise, and the leaner form shares HBM better
+    # packed, then CSR), then the smaller grid: such near-ties flip with noise, and the leaner
+    # form shares HBM better
     lean = {"kron": 0, "packed": 1}
     near = [(t, c) for t, c in final if t <= 1.03 * best_t]
-    best_t, best = min(near, key=lambda x: (min([lean[f] for f in lean if x[1].get(f)] + [2]), x[0]))
+    best_t, best = min(near, key=lambda x: (min([lean[f] for f in lean if x[1].get(f)] + [2]),
+                                            x[1].get("blocks_per_sm", 0), x[0]))
     del V0
     if verbose:
         for t, cfg in sorted(results, key=lambda x: x[0]):

@@ -188,7 +188,11 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         ++p_j;
         const int r0 = K.slab_off[sl];
         const int rows = K.slab_off[sl + 1] - r0;
-        const int nbox = (rows + KR_BOXR - 1) / KR_BOXR;
+        int nbox = (rows + KR_BOXR - 1) / KR_BOXR;
+        if (nbox * KR_BOXR > stage_rows) {  // a slab longer than max_rows: stage what fits, report it
+            atomicExch(err, 2);
+            nbox = stage_rows / KR_BOXR;
+        }
         const int st = (int)(issued % KR_NBUF);
         double2* dst = stages + st * stage_elems;
         mbar_expect_tx(&bar[st], (unsigned)(nbox * KR_BOXR * KR_CW * (int)sizeof(double2)));
@@ -215,7 +219,10 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
     bool bad = false;
     for (int s = blockIdx.x; s < K.nslab && !bad; s += gridDim.x) {
         const int off = K.slab_off[s];
-        const int R = K.slab_off[s + 1] - off;
+        const int Rs = K.slab_off[s + 1] - off;
+        // rows this block stages and holds; a slab longer than max_rows is reported, not read past
+        const int R = min(Rs, min(stage_rows, RPT * KR_NT));
+        if (tid == 0 && R != Rs) atomicExch(err, 2);
         const int m = K.slab_m[s];
         const uint32_t cfg = K.slab_cfg[s];
         const int bo = K.b_off[m];
@@ -269,7 +276,7 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
                             while (bits) {
                                 const int b = __ffs(bits) - 1;
                                 bits &= bits - 1u;
-                                const int rs = __ldg(nbr + b);
+                                const int rs = min((int)__ldg(nbr + b), stage_rows - 1);  // stays in the stage
                                 double2 t = T[b];
                                 if ((sa ^ __popc(B & ((1u << b) - 1u))) & 1) {
                                     t.x = -t.x;
@@ -325,46 +332,47 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
         }
         return;
     }
-    if (!LANCZOS) return;
-    // alpha partials: a fixed butterfly inside each warp, then the warps in order
+    if constexpr (LANCZOS) {
+        // alpha partials: a fixed butterfly inside each warp, then the warps in order
 #pragma unroll
-    for (int j = 0; j < KC; ++j) {
-        double v = apart[j];
+        for (int j = 0; j < KC; ++j) {
+            double v = apart[j];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) wred[warp][j] = v;
-    }
-    __syncthreads();
-    if (tid < kc) {
-        double t = 0.0;
-        for (int w = 0; w < NW; ++w) t += wred[w][tid];
-        S.part[(int64_t)blockIdx.x * k + c0 + tid] = t;
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) sh_last = atomicAdd(&tile_ticket[blockIdx.y], 1u) == gridDim.x - 1u;
-    __syncthreads();
-    if (!sh_last) return;
-    __threadfence();
-    __shared__ double red[KR_NT];
-    for (int j = 0; j < kc; ++j) {
-        const int col = c0 + j;
-        double t = 0.0;
-        for (int b = tid; b < (int)gridDim.x; b += KR_NT) t += __ldcg(S.part + (int64_t)b * k + col);
-        red[tid] = t;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) wred[warp][j] = v;
+        }
         __syncthreads();
-        for (int h = KR_NT / 2; h > 0; h >>= 1) {
-            if (tid < h) red[tid] += red[tid + h];
+        if (tid < kc) {
+            double t = 0.0;
+            for (int w = 0; w < NW; ++w) t += wred[w][tid];
+            S.part[(int64_t)blockIdx.x * k + c0 + tid] = t;
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) sh_last = atomicAdd(&tile_ticket[blockIdx.y], 1u) == gridDim.x - 1u;
+        __syncthreads();
+        if (!sh_last) return;
+        __threadfence();
+        __shared__ double red[KR_NT];
+        for (int j = 0; j < kc; ++j) {
+            const int col = c0 + j;
+            double t = 0.0;
+            for (int b = tid; b < (int)gridDim.x; b += KR_NT) t += __ldcg(S.part + (int64_t)b * k + col);
+            red[tid] = t;
+            __syncthreads();
+            for (int h = KR_NT / 2; h > 0; h >>= 1) {
+                if (tid < h) red[tid] += red[tid + h];
+                __syncthreads();
+            }
+            if (tid == 0) {
+                const double a = S.scur[col] * red[0];
+                S.alpha[col] = a;
+                if (S.active[col]) S.alpha_out[(int64_t)col * S.maxn + it] = a;
+            }
             __syncthreads();
         }
-        if (tid == 0) {
-            const double a = S.scur[col] * red[0];
-            S.alpha[col] = a;
-            if (S.active[col]) S.alpha_out[(int64_t)col * S.maxn + it] = a;
-        }
-        __syncthreads();
+        if (tid == 0) tile_ticket[blockIdx.y] = 0u;
     }
-    if (tid == 0) tile_ticket[blockIdx.y] = 0u;
 }
 
 // ---- host side ----------------------------------------------------------------------------
@@ -528,6 +536,7 @@ extern "C" int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double
     int h = 0;
     EDX_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     EDX_CUDA(cudaStreamSynchronize(st));
+    if (h == 2) return fail(EDX_ERR_INVALID, "edx_kron_spmm: the slab form is inconsistent (a slab longer than max_rows)");
     if (h) return fail(EDX_ERR_CUDA, "edx_kron_spmm: a staged slab load did not arrive within its time limit");
     return EDX_OK;
 }

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libedx.so")
 EDX_OK = 0
 EDX_C128, EDX_C64 = 0, 1
 EDX_HAM_I, EDX_HAM_N, EDX_TRANS_I, EDX_TRANS_F = 0, 1, 2, 3
+EDX_KRON_AUTO, EDX_KRON_STAGED, EDX_KRON_GATHER = 0, 1, 2  # slab product variants
 STATUS = {0: "EDX_OK", 1: "EDX_ERR_INVALID", 2: "EDX_ERR_CUDA", 3: "EDX_ERR_WORKSPACE",
           4: "EDX_ERR_ROW_CAPACITY", 5: "EDX_ERR_OVERFLOW"}
 

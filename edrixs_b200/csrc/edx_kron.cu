@@ -375,6 +375,197 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
     }
 }
 
+// ---- the slab product for large slabs: source rows read from global memory ---------------
+// When the largest slab does not fit the staged ring (more than about 590 rows of 128 bytes,
+// which is 12 or more bath orbitals), or on request, every thread owns one slab-order row
+// and the KC columns of its tile, finds its slab by a binary search of slab_off, and reads
+// its source rows where they lie: the row of the same rank for H_A and own-slab sources
+// (consecutive threads read consecutive rows), and per occupied (or empty) bath orbital the
+// row that the bath table names for hybridisation sources.  A slab is contiguous and a few MB
+// at most, so these reads mostly hit L2.  Grid (gx, column tiles of KC); block b owns rows
+// b * KR_NT + t, (b + gx) * KR_NT + t, ...  Epilogue and alpha partials as above.  A source
+// row outside its slab (an inconsistent slab form) is skipped and reported (err = 2).
+constexpr int KG_HOPS = 2;  // hops whose source rows load together
+
+template <int KC, bool LANCZOS>
+__global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron_gather(KronView K, int64_t nrows,
+                                                                     const double2* __restrict__ X,
+                                                                     double2* __restrict__ Y, KrylovState S, int k,
+                                                                     int it, unsigned* __restrict__ tile_ticket,
+                                                                     int* __restrict__ err) {
+    constexpr int NW = KR_NT / 32;
+    extern __shared__ double2 kg_tab[];  // t_cre, then t_ann (nah x nb each)
+    __shared__ double wred[NW][KC];
+    __shared__ bool sh_last;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int c0 = blockIdx.y * KC;
+    const int kc = min(KC, k - c0);
+    double2* tcre = kg_tab;
+    double2* tann = kg_tab + K.nah * K.nb;
+    for (int i = tid; i < K.nah * K.nb; i += KR_NT) {
+        tcre[i] = K.t_cre[i];
+        tann[i] = K.t_ann[i];
+    }
+    __syncthreads();
+    double bprev[KC], scur[KC], apart[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+        bprev[j] = scur[j] = apart[j] = 0.0;
+        if (LANCZOS && j < kc) {
+            bprev[j] = it > 0 ? S.beta[c0 + j] * S.sprev[c0 + j] : 0.0;
+            scur[j] = S.scur[c0 + j];
+        }
+    }
+    const uint32_t full = (1u << K.nb) - 1u;
+    bool bad = false;
+    for (int64_t i = (int64_t)blockIdx.x * KR_NT + tid; i < nrows; i += (int64_t)gridDim.x * KR_NT) {
+        int lo = 0, hi = K.nslab - 1;  // the last slab with slab_off <= i
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(K.slab_off + mid) <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        const int s = lo;
+        const int off = __ldg(K.slab_off + s);
+        const int r = (int)(i - off);
+        const int m = __ldg(K.slab_m + s);
+        const uint32_t cfg = __ldg(K.slab_cfg + s);
+        const int bo = __ldg(K.b_off + m);
+        const uint32_t B = __ldg(K.b_cfg + bo + r);
+        const uint16_t* nbr = K.b_nbr + (size_t)(bo + r) * K.nb;
+        double2 acc[KC];
+#pragma unroll
+        for (int j = 0; j < KC; ++j) acc[j] = make_double2(0.0, 0.0);
+        const int64_t se = __ldg(K.src_ptr + s + 1);
+        for (int64_t js = __ldg(K.src_ptr + s); js < se; ++js) {
+            const int sl = __ldg(K.src_slab + js);
+            const int kind = __ldg(K.src_kind + js);
+            const int type = kind & 15, q = kind >> 4;
+            const int soff = __ldg(K.slab_off + sl);
+            const int srows = __ldg(K.slab_off + sl + 1) - soff;
+            if (type <= EDX_KRON_SRC_OWN) {
+                if (r >= srows) {
+                    bad = true;
+                    continue;
+                }
+                double2 v = K.src_coef[js];
+                if (type == EDX_KRON_SRC_OWN) {
+                    const double2 d = __ldg(K.b_diag + bo + r);
+                    v.x += d.x;
+                    v.y += d.y;
+                }
+                const double2* xr = X + (int64_t)(soff + r) * k + c0;
+                double2 xs[KC];
+#pragma unroll
+                for (int j = 0; j < KC; ++j) xs[j] = j < kc ? ldx(xr + j) : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int j = 0; j < KC; ++j) acc[j] = fma_c(v, xs[j], acc[j]);
+            } else {
+                if (q >= K.nah) {
+                    bad = true;
+                    continue;
+                }
+                const bool cre = type == EDX_KRON_SRC_CRE;
+                const int a = __ldg(K.hyb_a + q);
+                const int sa = cre ? sig_cre(cfg, m, a, K.n_alo) : sig_ann(cfg, m, a, K.n_alo);
+                const double2* T = (cre ? tcre : tann) + q * K.nb;
+                uint32_t bits = cre ? B : (~B & full);
+                while (bits) {
+                    double2 t[KG_HOPS];
+                    int64_t row[KG_HOPS];
+                    bool ok[KG_HOPS];
+#pragma unroll
+                    for (int h = 0; h < KG_HOPS; ++h) {
+                        ok[h] = bits != 0u;
+                        const int b = ok[h] ? __ffs(bits) - 1 : 0;
+                        if (ok[h]) bits &= bits - 1u;
+                        const int rs = ok[h] ? (int)__ldg(nbr + b) : 0;
+                        if (rs >= srows) {
+                            bad = true;
+                            ok[h] = false;
+                        }
+                        row[h] = (int64_t)(soff + rs) * k + c0;
+                        t[h] = T[b];
+                        if ((sa ^ __popc(B & ((1u << b) - 1u))) & 1) {
+                            t[h].x = -t[h].x;
+                            t[h].y = -t[h].y;
+                        }
+                    }
+                    double2 xs[KG_HOPS][KC];
+#pragma unroll
+                    for (int h = 0; h < KG_HOPS; ++h)
+#pragma unroll
+                        for (int j = 0; j < KC; ++j)
+                            xs[h][j] = (ok[h] && j < kc) ? ldx(X + row[h] + j) : make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int h = 0; h < KG_HOPS; ++h)
+#pragma unroll
+                        for (int j = 0; j < KC; ++j) acc[j] = fma_c(t[h], xs[h][j], acc[j]);
+                }
+            }
+        }
+        const int64_t o = i * k + c0;
+#pragma unroll
+        for (int j = 0; j < KC; ++j) {
+            if (j < kc) {
+                if (LANCZOS) {
+                    const double2 vc = X[o + j];
+                    const double2 vp = Y[o + j];
+                    double2 w = make_double2(-bprev[j] * vp.x, -bprev[j] * vp.y);
+                    w.x = w.x + scur[j] * acc[j].x;
+                    w.y = w.y + scur[j] * acc[j].y;
+                    Y[o + j] = w;
+                    apart[j] += vc.x * w.x + vc.y * w.y;  // Re(conj(U_i) w); alpha = scur * sum
+                } else {
+                    Y[o + j] = acc[j];
+                }
+            }
+        }
+    }
+    if (bad) atomicExch(err, 2);
+    if constexpr (LANCZOS) {
+        // alpha partials: a fixed butterfly inside each warp, then the warps in order
+#pragma unroll
+        for (int j = 0; j < KC; ++j) {
+            double v = apart[j];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) wred[warp][j] = v;
+        }
+        __syncthreads();
+        if (tid < kc) {
+            double t = 0.0;
+            for (int w = 0; w < NW; ++w) t += wred[w][tid];
+            S.part[(int64_t)blockIdx.x * k + c0 + tid] = t;
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) sh_last = atomicAdd(&tile_ticket[blockIdx.y], 1u) == gridDim.x - 1u;
+        __syncthreads();
+        if (!sh_last) return;
+        __threadfence();
+        __shared__ double red[KR_NT];
+        for (int j = 0; j < kc; ++j) {
+            const int col = c0 + j;
+            double t = 0.0;
+            for (int b = tid; b < (int)gridDim.x; b += KR_NT) t += __ldcg(S.part + (int64_t)b * k + col);
+            red[tid] = t;
+            __syncthreads();
+            for (int h = KR_NT / 2; h > 0; h >>= 1) {
+                if (tid < h) red[tid] += red[tid + h];
+                __syncthreads();
+            }
+            if (tid == 0) {
+                const double a = S.scur[col] * red[0];
+                S.alpha[col] = a;
+                if (S.active[col]) S.alpha_out[(int64_t)col * S.maxn + it] = a;
+            }
+            __syncthreads();
+        }
+        if (tid == 0) tile_ticket[blockIdx.y] = 0u;
+    }
+}
+
 // ---- host side ----------------------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
     static std::once_flag once;
@@ -422,7 +613,22 @@ int kron_check(const edx_kron* K) {
     return EDX_OK;
 }
 
-int kron_grid_x(const edx_kron* K, int k, int /*col_group*/) {
+// the staged product needs every slab within one block (4 rows per thread at most) and the
+// ring of staged slabs within shared memory
+static bool staged_fits(const edx_kron* K) { return rpt_of(K) != 0 && smem_bytes(K) <= 227 * 1024; }
+static bool gather_of(const edx_kron* K, int variant) { return variant == EDX_KRON_GATHER || !staged_fits(K); }
+// columns per thread of the gather product: the smallest supported count >= k, 8 beyond
+static int gather_kc(int k) { return kc_of(k); }
+
+int kron_grid_x(const edx_kron* K, int k, int variant) {
+    if (gather_of(K, variant)) {
+        const int kc = gather_kc(k);
+        const int ntile = (k + kc - 1) / kc;
+        const int64_t target = (int64_t)num_sms() * 8 * 4;  // 8 blocks of 256 threads per SM, 4 rounds
+        const int64_t gx = (target + ntile - 1) / ntile;
+        const int64_t need = (K->nrows + KR_NT - 1) / KR_NT;
+        return (int)std::max<int64_t>(1, std::min(gx, need));
+    }
     const size_t sm = smem_bytes(K);
     int occ = (int)std::min<size_t>(8, (size_t)(227 * 1024) / std::max<size_t>(sm + 2048, 1));
     if (occ < 1) occ = 1;
@@ -476,9 +682,34 @@ static int launch_kron_kc(const edx_kron* K, const CUtensorMap* tm, const double
                 4 * KR_NT);
 }
 
+template <int KC, bool LANCZOS>
+static int launch_gather_kc(const edx_kron* K, const double2* X, double2* Y, const KrylovState& S, int k, int it,
+                            unsigned* tt, int* err, cudaStream_t st) {
+    auto kern = k_lanczos_apply_kron_gather<KC, LANCZOS>;
+    const size_t sm = 2 * (size_t)K->nah * K->nb * sizeof(double2);
+    const int ntile = (k + KC - 1) / KC;
+    EDX_REQUIRE(ntile <= 65535, "slab form: too many column tiles");
+    dim3 grid(kron_grid_x(K, k, EDX_KRON_GATHER), ntile);
+    kern<<<grid, KR_NT, sm, st>>>(view_of(K), K->nrows, X, Y, S, k, it, tt, err);
+    EDX_CHECK_LAUNCH();
+    return EDX_OK;
+}
+
 template <bool LANCZOS>
 static int launch_kron(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
-                       int k, int it, unsigned* tt, int* err, cudaStream_t st) {
+                       int k, int it, unsigned* tt, int* err, int variant, cudaStream_t st) {
+    if (variant == EDX_KRON_STAGED && !staged_fits(K))
+        return fail(EDX_ERR_INVALID, "slab form: slabs of %d rows do not fit the staged product's shared memory",
+                    K->max_rows);
+    if (gather_of(K, variant)) {
+        switch (gather_kc(k)) {
+        case 1: return launch_gather_kc<1, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
+        case 2: return launch_gather_kc<2, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
+        case 4: return launch_gather_kc<4, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
+        case 6: return launch_gather_kc<6, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
+        default: return launch_gather_kc<8, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
+        }
+    }
     switch (kc_of(k)) {
     case 1: return launch_kron_kc<1, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
     case 2: return launch_kron_kc<2, LANCZOS>(K, tm, X, Y, S, k, it, tt, err, st);
@@ -488,11 +719,16 @@ static int launch_kron(const edx_kron* K, const CUtensorMap* tm, const double2* 
     }
 }
 
-int kron_col_group(int /*k*/, int /*requested*/) { return KR_CW; }
+// the product variant a caller's apply_col_group selects (EDX_KRON_AUTO / _STAGED / _GATHER;
+// other values: automatic)
+int kron_col_group(int /*k*/, int requested) {
+    return (requested == EDX_KRON_STAGED || requested == EDX_KRON_GATHER) ? requested : EDX_KRON_AUTO;
+}
 
 int apply_kron(const edx_kron* K, const void* tmap, const double2* Vc, double2* Vp, const KrylovState& S, int it,
                unsigned* tile_ticket, int* err, int col_group, cudaStream_t st) {
-    return launch_kron<true>(K, static_cast<const CUtensorMap*>(tmap), Vc, Vp, S, S.k, it, tile_ticket, err, st);
+    return launch_kron<true>(K, static_cast<const CUtensorMap*>(tmap), Vc, Vp, S, S.k, it, tile_ticket, err,
+                             kron_col_group(S.k, col_group), st);
 }
 
 __global__ void k_permute_rows(int64_t n, int k, const double2* __restrict__ src, int64_t lds,
@@ -520,23 +756,23 @@ extern "C" int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double
     int rc = kron_check(K);
     if (rc) return rc;
     EDX_REQUIRE(k >= 1 && d_x && d_y && d_x != d_y, "edx_kron_spmm: bad arguments");
-    (void)col_group;  // the slab product always works on 8-column tiles
-    const int cw = KR_CW;
+    const int variant = kron_col_group(k, col_group);
     Workspace w(d_work, work_bytes);
     int* err = w.take<int>(1);
     if (!err) return fail(EDX_ERR_WORKSPACE, "edx_kron_spmm: workspace too small");
     cudaStream_t st = as_stream(stream);
     EDX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
     alignas(64) CUtensorMap tm;
-    if ((rc = kron_tensor_map(K, reinterpret_cast<const double2*>(d_x), k, cw, &tm))) return rc;
+    if (!gather_of(K, variant) && (rc = kron_tensor_map(K, reinterpret_cast<const double2*>(d_x), k, 0, &tm)))
+        return rc;
     KrylovState S{};
     rc = launch_kron<false>(K, &tm, reinterpret_cast<const double2*>(d_x), reinterpret_cast<double2*>(d_y), S, k, 0,
-                            nullptr, err, st);
+                            nullptr, err, variant, st);
     if (rc) return rc;
     int h = 0;
     EDX_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     EDX_CUDA(cudaStreamSynchronize(st));
-    if (h == 2) return fail(EDX_ERR_INVALID, "edx_kron_spmm: the slab form is inconsistent (a slab longer than max_rows)");
+    if (h == 2) return fail(EDX_ERR_INVALID, "edx_kron_spmm: the slab form is inconsistent (a slab or a source row out of range)");
     if (h) return fail(EDX_ERR_CUDA, "edx_kron_spmm: a staged slab load did not arrive within its time limit");
     return EDX_OK;
 }

@@ -1063,7 +1063,7 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
             EDX_CUDA(cudaStreamSynchronize(st));
             if (h[2]) {
                 drop_events();
-                if (h[2] == 2) return fail(EDX_ERR_INVALID, "edx_krylov: the slab form is inconsistent (a slab longer than max_rows)");
+                if (h[2] == 2) return fail(EDX_ERR_INVALID, "edx_krylov: the slab form is inconsistent (a slab or a source row out of range)");
                 return fail(EDX_ERR_CUDA, "edx_krylov: a staged slab load did not arrive within its time limit");
             }
             if (h[0] == 0) break;

@@ -16,6 +16,7 @@ from ._lib import BuildDesc, Csr, KrylovOpts, Kron, Packed, call
 
 C128, C64 = _lib.EDX_C128, _lib.EDX_C64
 HAM_I, HAM_N, TRANS_I, TRANS_F = _lib.EDX_HAM_I, _lib.EDX_HAM_N, _lib.EDX_TRANS_I, _lib.EDX_TRANS_F
+KRON_AUTO, KRON_STAGED, KRON_GATHER = _lib.EDX_KRON_AUTO, _lib.EDX_KRON_STAGED, _lib.EDX_KRON_GATHER
 
 
 def _stream():

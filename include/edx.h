@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define EDX_ABI_VERSION 5
+#define EDX_ABI_VERSION 6
 
 /* status codes */
 #define EDX_OK 0
@@ -224,11 +224,20 @@ typedef struct edx_kron {
     const double* b_diag;       /* device complex128[2^nb] */
 } edx_kron;
 
-/* Y = H X in slab order for k columns (row-major, ld = k), on the slab form.  The source
+/* Variants of the slab product (the col_group argument of edx_kron_spmm, apply_col_group of
+ * edx_krylov_opts with apply_kron; other values mean EDX_KRON_AUTO).  STAGED: the source
  * slabs are staged in shared memory by the tensor-memory accelerator (2-D tiled loads of
- * 32-row boxes; no multicast).  col_group: columns per block (1, 2, 4, 6, 8, 12 or 16;
- * 0 = the smallest >= k, 16 beyond).  EDX_ERR_CUDA if a staged load did not arrive within
- * its time limit (the kernel records it in the workspace).  X and Y must not overlap. */
+ * 32-row boxes; no multicast); it needs slabs of at most 1024 rows whose ring of three
+ * staged slabs fits in shared memory (about 590 rows: up to 11 bath orbitals).  GATHER: every
+ * thread reads its row's source rows from global memory (any slab size).  AUTO: STAGED when
+ * it fits, else GATHER. */
+#define EDX_KRON_AUTO 0
+#define EDX_KRON_STAGED 1
+#define EDX_KRON_GATHER 2
+/* Y = H X in slab order for k columns (row-major, ld = k), on the slab form, in the variant
+ * col_group selects (above).  EDX_ERR_CUDA if a staged load did not arrive within its time
+ * limit; EDX_ERR_INVALID if a slab or a source row lies outside the descriptor's ranges (the
+ * kernels record both in the workspace and skip the access).  X and Y must not overlap. */
 int edx_kron_spmm_workspace(size_t* bytes);
 int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double* d_y, int col_group, void* d_work,
                   size_t work_bytes, void* stream);
@@ -309,7 +318,8 @@ typedef struct edx_krylov_opts {
      * one 32-bit word per off-diagonal entry and the value from a table in shared memory,
      * with the launch-shape fields above. */
     const edx_packed* apply_packed;
-    /* slab form of the same matrix, or NULL.  With it the product is k_lanczos_apply_kron:
+    /* slab form of the same matrix, or NULL.  With it the product is k_lanczos_apply_kron
+     * (or k_lanczos_apply_kron_gather: apply_col_group selects the EDX_KRON_* variant):
      * the start vectors d_v0 and every Lanczos vector are in slab order, and A is used for
      * its shape only.  Projections need operators whose columns are in slab order too. */
     const edx_kron* apply_kron;

@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=50.0, help="offered arrivals per second")
     ap.add_argument("--serve-seed", type=int, default=7)
     ap.add_argument("--serve-workers", type=int, default=3)
+    ap.add_argument("--serve-norb-max", type=int, default=26,
+                    help="largest model of the serving mix (valence spin-orbitals, 16..26)")
     ap.add_argument("--hbm-budget", type=float, default=150e9)
     ap.add_argument("--scale", action="store_true",
                     help="XAS and RIXS at scale: 10 + 16 orbitals, N = 13 (10.4 M ground, 57.9 M intermediate "
@@ -801,8 +803,9 @@ def run_ed(args):
 
 def serve_mix(args):
     """The serving mix: seeded Poisson arrivals (rate --serve-rate) of ED, XAS and RIXS jobs on
-    impurity models of 16 to 22 valence spin-orbitals (10 d + 6..12 bath), N = norb/2 - 1 ..
-    norb/2 + 1, so Hilbert spaces of 1e4 to 4e6 states; 20 % of the jobs are RIXS or XAS on a
+    impurity models of 16 to --serve-norb-max (26) valence spin-orbitals (10 d + 6..16 bath,
+    every size equally likely), N = norb/2 - 1 .. norb/2 + 1, so initial sectors of 1e4 to
+    1e7 states and intermediate sectors up to 6e7; 20 % of the jobs are RIXS or XAS on a
     Hamiltonian an earlier job used, with new incident energies or polarisations."""
     from edrixs_b200.serve import ModelSpec, Request
     rng = np.random.default_rng(args.serve_seed)
@@ -815,7 +818,7 @@ def serve_mix(args):
             kind = "rixs" if rng.random() < 0.5 else "xas"
         else:
             kind = rng.choice(["ed", "xas", "rixs"], p=[0.4, 0.3, 0.3])
-            nbath = int(rng.choice([6, 8, 10] if kind == "rixs" else [6, 8, 10, 12]))
+            nbath = int(rng.integers(6, args.serve_norb_max - 10 + 1))
             norb = 10 + nbath
             spec = ModelSpec(nbath, norb // 2 + int(rng.integers(-1, 2)), int(rng.integers(1, 10 ** 6)))
             used.append(spec)
@@ -1032,7 +1035,7 @@ def run_serve(args):
                 f.result(timeout=1800)
             except Exception as e:
                 failed += 1
-                key = f"{req.kind}: {type(e).__name__}: {str(e)[:160]}"
+                key = f"{req.kind} norb {10 + req.model.nbath} N {req.model.nelec}: {type(e).__name__}: {str(e)[:160]}"
                 errors[key] = errors.get(key, 0) + 1
         makespan = time.perf_counter() - t0
     finally:
@@ -1050,6 +1053,7 @@ def run_serve(args):
         sk = np.array([r["service_s"] for r in rk]) * 1e3
         by_kind[kind] = {"n": len(rk), "p50_ms": pct(lk, 50), "p99_ms": pct(lk, 99), "service_p50_ms": pct(sk, 50)}
     dims = [math.comb(10 + r.model.nbath, r.model.nelec) for _, r in jobs]
+    dims_n = [6 * math.comb(10 + r.model.nbath, r.model.nelec + 1) for _, r in jobs if r.kind != "ed"]
     line = {"metric": "serving mix: completed requests/s & p50/p99 latency (queueing + service)",
             "value": round(len(recs) / makespan, 3), "unit": "req/s", "higher_is_better": True, "n_gpus": 1,
             "n_requests": len(jobs), "completed": len(recs), "failed": failed, "errors": errors,
@@ -1057,8 +1061,9 @@ def run_serve(args):
             "latency_ms": {"p50": pct(lat, 50), "p99": pct(lat, 99)}, "by_kind": by_kind,
             "coalesced_requests": int(sum(1 for r in recs if r["coalesced"] > 1)),
             "dtype": "c128", "data": "synthetic (seeded SIAM inputs; reference atomic tensors)",
-            "config": {"workload": "ED/XAS/RIXS serving mix, norb 16-22, N = norb/2 +- 1, "
-                                   f"dim_i {min(dims)}..{max(dims)}, 20 % reuse of a resident Hamiltonian",
+            "config": {"workload": f"ED/XAS/RIXS serving mix, norb 16-{args.serve_norb_max}, N = norb/2 +- 1, "
+                                   f"dim_i {min(dims)}..{max(dims)}, dim_n up to {max(dims_n)}, "
+                                   "20 % reuse of a resident Hamiltonian",
                        "hbm_budget_gb": args.hbm_budget / 1e9, "workers": args.serve_workers,
                        "seed": args.serve_seed}}
     print(json.dumps(line), flush=True)

@@ -452,10 +452,10 @@ static int pack_terms(const edx_build_desc* d, const BuildWs& w, cudaStream_t st
     return EDX_OK;
 }
 
-static int cap_warps(int cap) {
-    int w = 131072 / (cap * 8);
-    return std::max(1, std::min(8, w));
+constexpr int cap_warps_c(int cap) {
+    return 131072 / (cap * 8) < 1 ? 1 : (131072 / (cap * 8) > 8 ? 8 : 131072 / (cap * 8));
 }
+static int cap_warps(int cap) { return cap_warps_c(cap); }
 
 template <int CAP, bool FILL>
 static int launch_cap(const BuildK& p, int32_t* row_nnz, const int64_t* row_ptr, int32_t* col,
@@ -465,7 +465,12 @@ static int launch_cap(const BuildK& p, int32_t* row_nnz, const int64_t* row_ptr,
     tab_words = (tab_words + 1) & ~size_t(1);
     size_t smem = (tab_words + (size_t)warps * CAP) * sizeof(uint64_t);
     auto kern = k_build<CAP, FILL>;
-    EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the attribute is the largest this instantiation can ask for (a 64 x 64 ranking table,
+    // search_norb <= 63), the same on every call: threads that build different bases at once
+    // must not lower it between another thread's setting and its launch
+    constexpr size_t smem_max = (64 * 64 + (size_t)cap_warps_c(CAP) * CAP) * sizeof(uint64_t);
+    static_assert(smem_max <= 227 * 1024, "build: shared memory");
+    EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
     int64_t blocks = (p.nrows + warps - 1) / warps;
     int maxb = num_sms() * std::max(1, 16 / warps) * 2;
     if (blocks > maxb) blocks = maxb;

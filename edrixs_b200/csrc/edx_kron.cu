@@ -615,7 +615,7 @@ int kron_check(const edx_kron* K) {
 
 // the staged product needs every slab within one block (4 rows per thread at most) and the
 // ring of staged slabs within shared memory
-static bool staged_fits(const edx_kron* K) { return rpt_of(K) != 0 && smem_bytes(K) <= 227 * 1024; }
+static bool staged_fits(const edx_kron* K) { return rpt_of(K) != 0 && smem_bytes(K) + 8 * 1024 <= 227 * 1024; }
 static bool gather_of(const edx_kron* K, int variant) { return variant == EDX_KRON_GATHER || !staged_fits(K); }
 // columns per thread of the gather product: the smallest supported count >= k, 8 beyond
 static int gather_kc(int k) { return kc_of(k); }
@@ -660,8 +660,17 @@ static int launch_kron_rpt(const edx_kron* K, const CUtensorMap* tm, const doubl
                            int k, int it, unsigned* tt, int* err, cudaStream_t st) {
     auto kern = k_lanczos_apply_kron<KC, RPT, LANCZOS>;
     const size_t sm = smem_bytes(K);
-    EDX_REQUIRE(sm <= 227 * 1024, "slab form: %zu bytes of staged slabs exceed shared memory", sm);
-    EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    // the attribute is the most this kernel can be given (the device's opt-in limit less its
+    // static shared memory), the same on every call: threads launching for different slab
+    // forms at once must not lower it under one another's launch
+    int dev = 0, optin = 0;
+    EDX_CUDA(cudaGetDevice(&dev));
+    EDX_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    EDX_CUDA(cudaFuncGetAttributes(&fa, kern));
+    const size_t max_dyn = (size_t)optin - fa.sharedSizeBytes;
+    EDX_REQUIRE(sm <= max_dyn, "slab form: %zu bytes of staged slabs exceed shared memory", sm);
+    EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn));
     const int ntile = (k + KR_CW - 1) / KR_CW;
     EDX_REQUIRE(ntile <= 65535, "slab form: too many column tiles");
     dim3 grid(kron_grid_x(K, k, 0), ntile);

@@ -339,7 +339,7 @@ def kron_form(mode, basis: Basis, hopping, coulomb=None, num_val_orbs=0, num_cor
     from . import kron
     if mode not in (HAM_I, HAM_N):
         return None
-    spec = kron.kron_spec(hopping, coulomb, basis.states.cpu().numpy(), "ham_i" if mode == HAM_I else "ham_n",
+    spec = kron.kron_spec(hopping, coulomb, basis.states, "ham_i" if mode == HAM_I else "ham_n",
                           num_val_orbs=num_val_orbs, num_core_orbs=num_core_orbs)
     if spec is None:
         return None

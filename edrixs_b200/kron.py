@@ -97,7 +97,7 @@ class KronSpec:
     b_diag: np.ndarray     # complex128[2^nb] bath-level energy of each configuration
     a_hop: tuple           # A-terms (idx, val) of the hopping list
     a_coul: tuple          # A-terms (idx, val) of the Coulomb list
-    perm: np.ndarray       # int64[n] reference row of each slab row
+    perm: object           # int64[n] reference row of each slab row (numpy, or a tensor on the basis's device)
 
     @property
     def nslab(self):
@@ -112,13 +112,60 @@ class KronSpec:
         return int(np.diff(self.slab_off).max())
 
 
+def _slab_perm_host(full, m, sizes, slab_off, b_cfg, b_off, b0, nv, kidx, basis):
+    """Reference row of every slab row: slab s, rank r is the state with A bits full[s] and
+    bath configuration b_cfg[b_off[m[s]] + r] at bit b0; its row is the valence state's index
+    in the ascending basis (times the core-hole index k, k-major, when kidx is given).  None
+    when a state is missing from the basis or two slab rows meet one reference row."""
+    n_rows = int(slab_off[-1])
+    srow = np.repeat(np.arange(len(full)), sizes)
+    rank = np.arange(n_rows) - slab_off[srow]
+    full_row = full[srow] | (b_cfg[b_off[m[srow]] + rank] << b0)
+    val = full_row & ((1 << nv) - 1)
+    vidx = np.searchsorted(basis, val)
+    if np.any(vidx >= len(basis)) or np.any(basis[np.minimum(vidx, len(basis) - 1)] != val):
+        return None
+    perm = kidx[full_row >> nv] * len(basis) + vidx if kidx is not None else vidx
+    if np.bincount(perm, minlength=n_rows).max() != 1:
+        return None
+    return perm
+
+
+def _slab_perm_device(full, m, sizes, slab_off, b_cfg, b_off, b0, nv, kidx, basis):
+    """_slab_perm_host on the basis tensor's device (tens of millions of rows in milliseconds
+    instead of a minute on the host); returns a device int64 tensor."""
+    import torch
+    dev = basis.device
+
+    def t(a):
+        return torch.as_tensor(np.ascontiguousarray(a, dtype=np.int64), device=dev)
+
+    n_rows = int(slab_off[-1])
+    srow = torch.repeat_interleave(torch.arange(len(full), device=dev), t(sizes))
+    rank = torch.arange(n_rows, device=dev) - t(slab_off)[srow]
+    full_row = t(full)[srow] | (t(b_cfg)[t(b_off)[t(m)[srow]] + rank] << b0)
+    del srow, rank
+    val = full_row & ((1 << nv) - 1)
+    vidx = torch.searchsorted(basis, val)
+    if bool((vidx >= len(basis)).any()) or bool((basis[vidx.clamp(max=len(basis) - 1)] != val).any()):
+        return None
+    del val
+    perm = t(kidx)[full_row >> nv] * len(basis) + vidx if kidx is not None else vidx
+    del full_row
+    if int(torch.bincount(perm, minlength=n_rows).max()) != 1:
+        return None
+    return perm
+
+
 def kron_spec(hopping, coulomb, basis_states, mode="ham_i", num_val_orbs=0, num_core_orbs=0, min_nb=4):
     """The slab form of the Hamiltonian built from these terms over this basis, or None.
 
     hopping / coulomb: (idx int[n, 2 or 4] 1-based, val complex[n]) as read from the *.in files
     (src/io.f90:93-152); basis_states: the valence Fock basis of the matrix (ascending);
     mode: "ham_i" (rows = basis states) or "ham_n" (rows = core-hole configuration k x basis
-    state, k-major, src/ham.f90:414-446, with num_core_orbs core orbitals above the valence)."""
+    state, k-major, src/ham.f90:414-446, with num_core_orbs core orbitals above the valence).
+    basis_states may be a device tensor (int64): the row permutation is then computed on its
+    device and ``perm`` is a device tensor."""
     hi = np.asarray(hopping[0], dtype=np.int64).reshape(-1, 2) - 1 if hopping is not None else np.zeros((0, 2), int)
     hv = np.asarray(hopping[1], dtype=np.complex128).reshape(-1) if hopping is not None else np.zeros(0, complex)
     ci = np.asarray(coulomb[0], dtype=np.int64).reshape(-1, 4) - 1 if coulomb is not None else np.zeros((0, 4), int)
@@ -128,7 +175,8 @@ def kron_spec(hopping, coulomb, basis_states, mode="ham_i", num_val_orbs=0, num_
         return None
     if mode == "ham_i":
         nc = 0
-    basis = np.asarray(basis_states, dtype=np.int64)
+    on_device = not isinstance(basis_states, np.ndarray) and hasattr(basis_states, "device")
+    basis = basis_states if on_device else np.asarray(basis_states, dtype=np.int64)
     if nv <= 0 or len(basis) == 0:
         return None
     nval_e = bin(int(basis[0])).count("1")
@@ -230,25 +278,14 @@ def kron_spec(hopping, coulomb, basis_states, mode="ham_i", num_val_orbs=0, num_
             else:
                 up[s, q] = pos.get(int(c | (1 << a)), -1)
     # permutation: slab row -> reference row
-    srow = np.repeat(np.arange(len(cfgs)), sizes)
-    rank = np.arange(n_rows) - slab_off[srow]
-    bcfg_row = b_cfg[b_off[m[srow]] + rank]
-    full_row = full[srow] | (bcfg_row << b0)
-    val = full_row & ((1 << nv) - 1)
-    vidx = np.searchsorted(basis, val)
-    if np.any(vidx >= len(basis)) or np.any(basis[np.minimum(vidx, len(basis) - 1)] != val):
-        return None
-    if mode == "ham_n":
-        core = full_row >> nv
-        # fock_core(k) = 2^nc - 1 - 2^(nc-k) has its hole on core orbital nc - k (k = 1..nc,
-        # src/ham.f90:419-421); every slab has exactly one hole
-        kidx = np.zeros(1 << nc, dtype=np.int64)
-        for h in range(nc):
-            kidx[((1 << nc) - 1) ^ (1 << h)] = nc - 1 - h
-        perm = kidx[core] * len(basis) + vidx
-    else:
-        perm = vidx
-    if len(np.unique(perm)) != n_rows:
+    # fock_core(k) = 2^nc - 1 - 2^(nc-k) has its hole on core orbital nc - k (k = 1..nc,
+    # src/ham.f90:419-421); every slab has exactly one hole
+    kidx = np.zeros(1 << nc, dtype=np.int64)
+    for h in range(nc):
+        kidx[((1 << nc) - 1) ^ (1 << h)] = nc - 1 - h
+    perm = (_slab_perm_device if on_device else _slab_perm_host)(full, m, sizes, slab_off, b_cfg, b_off, b0, nv,
+                                                                 kidx if mode == "ham_n" else None, basis)
+    if perm is None:
         return None
     return KronSpec(n=n_rows, nb=nb, b0=int(b0), a_bits=a_bits, n_alo=n_alo,
                     slab_cfg=cfgs.astype(np.uint32), slab_full=full, slab_m=m.astype(np.int32),

@@ -56,7 +56,7 @@ class RixsProblem:
 
     def nbytes(self):
         b = self.Hn.nbytes() + self.Hf.nbytes() + sum(D.nbytes() for D in self.Din + self.Dout)
-        if self.Hn.val64 is not None:
+        if getattr(self.Hn, "val64", None) is not None:
             b += self.Hn.nnz * 8
         b += sum(M.nbytes() for M in self.packed.values())
         b += sum(M.nbytes() for M in self.kron.values())

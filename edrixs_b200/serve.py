@@ -1,8 +1,12 @@
 """Continuous-batching request loop for ED / XAS / RIXS jobs on one GPU.
 
 * Requests name a Hamiltonian by its generating parameters (``ModelSpec``); the server keeps
-  each Hamiltonian's CSR matrices, transition operators and ground states resident in HBM
-  (``Resident``) and reuses them for later requests.
+  each Hamiltonian's product form, transition operators and ground states resident in HBM
+  (``Resident``) and reuses them for later requests.  The product form is the packed matrix
+  (its CSR is dropped once packed), or, for intermediate sectors above SLAB_ONLY_ROWS rows,
+  the slab form alone: no CSR is built at all (at 58 M rows the CSR takes 114 GB while it is
+  packed, the packed form 35 GB, the slab form 0.9 GB, and the slab product runs the
+  few-column recurrences as fast as the packed one).
 * Admission: a request starts when its estimated device footprint (its resident problem if
   not cached yet + its solve working set) fits in the HBM budget next to everything in
   flight; idle residents are evicted least-recently-used to make room.  Requests that do
@@ -69,8 +73,41 @@ class Request:
 _ids = itertools.count()
 
 
+# intermediate sectors above this many rows are held in the slab form alone (when the model
+# has one); below it the packed form, whose product is about 15 % faster at 1 M rows
+SLAB_ONLY_ROWS = 20_000_000
+# rows below which the CSR itself is kept (the eigensolver's dense path needs it)
+SMALL_ROWS = 4096
+# bytes per row, for the admission estimate: a complex128 CSR while it is built and packed
+# (up to ~100 entries per row at 26 orbitals), its packed form, the slab form (row
+# permutation, its inverse and tables) and the transient of building the slab form
+CSR_ROW, PACKED_ROW, SLAB_ROW, SLAB_BUILD_ROW = 2048 + 640, 640, 24, 64
+# basis vectors of the ground-state eigensolver (block thick-restart Lanczos)
+ED_BASIS = 64
+# final-state Lanczos columns per launch in the server (bounds its working set)
+FINAL_BLOCK = 64
+# Lanczos vectors folded at a time into the final-state start vectors (streamed RIXS)
+STREAM_WINDOW = 4
+
+
+def _product_form(mode, basis, hop, coul, nv, nc, slab_first):
+    """The matrix a resident keeps for products: the slab form when slab_first and the model
+    has one (no CSR is built), else the packed form with its CSR dropped, else (too many
+    distinct values, or a small matrix) the CSR."""
+    if slab_first:
+        K = device.kron_form(mode, basis, hop, coul, num_val_orbs=nv, num_core_orbs=nc)
+        if K is not None:
+            return K
+    H = device.build_csr(mode, basis, hop, coul, num_val_orbs=nv, num_core_orbs=nc)
+    if H.nrows < SMALL_ROWS:
+        return H
+    P = device.pack(H)
+    return P if P is not None else H
+
+
 class Resident:
-    """Device state of one Hamiltonian, built on first use."""
+    """Device state of one Hamiltonian, built on first use.  Hi / Hn: the product form of
+    H_i and H_n (device.PackedMatrix, device.KronMatrix or device.CSR, see _product_form)."""
 
     def __init__(self, spec: ModelSpec):
         self.spec = spec
@@ -84,15 +121,12 @@ class Resident:
         self.gs_v = None
         self.edge = None
         self.ops = {}
-        self.packed = {}             # "hi" / "hn" -> device.PackedMatrix (None: too many values)
-        self.kron = {}               # "hi" / "hn" -> device.KronMatrix (None: no impurity x bath form)
         self.busy = 0
         self.last_used = time.monotonic()
 
     def nbytes(self):
         b = 0
-        for M in [self.Hi, self.Hn] + list(self.ops.values()) + list(self.packed.values()) + \
-                list(self.kron.values()):
+        for M in [self.Hi, self.Hn] + list(self.ops.values()):
             if M is not None:
                 b += M.nbytes()
         if self.gs_v is not None:
@@ -112,22 +146,24 @@ class Resident:
                                   hop_n=rt(siam.nonzero_terms(m.emat_n), 2), coul_n=rt(siam.nonzero_terms(m.umat_n), 4))
             if self.Hi is None:
                 self.bi = device.fock_unrank(s.nv, s.nelec)
-                self.Hi = device.build_csr(device.HAM_I, self.bi, self.terms["hop_i"], self.terms["coul_i"],
-                                           num_val_orbs=s.nv)
-                self.packed["hi"] = device.pack(self.Hi)
-                self.kron["hi"] = device.kron_form(device.HAM_I, self.bi, self.terms["hop_i"], self.terms["coul_i"],
-                                                   num_val_orbs=s.nv)
+                self.Hi = _product_form(device.HAM_I, self.bi, self.terms["hop_i"], self.terms["coul_i"], s.nv, 0,
+                                        slab_first=False)
             if self.gs_v is None or self.gs_v.shape[1] < ngs:
-                e, v = solvers.lowest_eigs(self.Hi, ngs, ngs, tol=1e-9, packed=self.packed.get("hi"))
+                # two guard vectors in the block: a level just above the wanted ones (a
+                # near-degenerate pair across the boundary) otherwise stalls their residuals
+                e, v = solvers.lowest_eigs(self.Hi, ngs, ngs, tol=1e-9, block=min(ngs + 2, 6), mmax=ED_BASIS)
                 self.gs_e, self.gs_v = np.asarray(e), v.contiguous()
             if need_n and self.Hn is None:
                 self.bn = device.fock_unrank(s.nv, s.nelec + 1)
-                self.Hn = device.build_csr(device.HAM_N, self.bn, self.terms["hop_n"], self.terms["coul_n"],
-                                           num_val_orbs=s.nv, num_core_orbs=6)
-                self.packed["hn"] = device.pack(self.Hn)
-                self.kron["hn"] = device.kron_form(device.HAM_N, self.bn, self.terms["hop_n"], self.terms["coul_n"],
-                                                   num_val_orbs=s.nv, num_core_orbs=6)
-                e_n, _ = solvers.lowest_eigs(self.Hn, 1, 1, tol=1e-6, packed=self.packed.get("hn"))
+                nn = 6 * self.bn.ndim
+                self.Hn = _product_form(device.HAM_N, self.bn, self.terms["hop_n"], self.terms["coul_n"], s.nv, 6,
+                                        slab_first=nn > SLAB_ONLY_ROWS)
+                if isinstance(self.Hn, device.KronMatrix):
+                    # the absorption edge from a plain Lanczos run (a few vectors, not the
+                    # block eigensolver's basis of tens of GB at this size)
+                    e_n, _ = solvers.plain_lanczos_eigs(self.Hn, 1, 0, 400, 1e-9)
+                else:
+                    e_n, _ = solvers.lowest_eigs(self.Hn, 1, 1, tol=1e-6)
                 self.edge = float(e_n[0] - self.gs_e[0])
             # the resident is shared with other workers' streams: finish building it here
             torch.cuda.current_stream().synchronize()
@@ -162,20 +198,56 @@ def _dims(spec: ModelSpec):
     return ni, nn
 
 
-def estimate_bytes(req: Request, resident_cached: bool):
-    """Upper estimate of the device bytes a request needs (resident part + working set)."""
+def _rixs_shape(req: Request):
+    """(k, npout, K): Lanczos columns on H_n (incident polarisations x ground states),
+    outgoing polarisations, final-state columns."""
+    npin = len(set(siam_pol_in(p) for p in req.pols))
+    npout = len(set(siam_pol_out(p) for p in req.pols))
+    k = npin * req.ngs
+    return k, npout, npout * k * len(req.omegas)
+
+
+def rixs_streamed(req: Request, budget):
+    """Whether the server runs this RIXS request in the streamed form (D_out^+ v_i folded into
+    the final-state start vectors as the Lanczos vectors appear) rather than storing every
+    projected vector: when storing them would take more than a quarter of the HBM budget."""
+    ni, _ = _dims(req.model)
+    k, npout, _ = _rixs_shape(req)
+    return npout * k * req.linsys_max * ni * 16 > budget / 4
+
+
+def estimate_bytes(req: Request, resident_cached: bool, budget=150e9):
+    """Upper estimate of the device bytes a request needs: its resident problem when not
+    cached yet (the product forms it keeps, plus the larger of the build transients: a CSR
+    while it is packed, or the slab form's row tables, and the edge's eigensolver basis) and
+    the working set of its solve."""
     ni, nn = _dims(req.model)
-    per_row = 24 * 80  # ~80 nonzeros per row at 20 bytes + slack
-    resident = 0 if resident_cached else (ni + (nn if req.kind != "ed" else 0)) * per_row
+    resident = 0
+    if not resident_cached:
+        keep = ni * PACKED_ROW
+        peak = ni * CSR_ROW + (ED_BASIS + 8) * ni * 16  # build of H_i, then the ground-state basis
+        if req.kind != "ed":
+            if nn > SLAB_ONLY_ROWS:
+                keep += nn * SLAB_ROW
+                peak = max(peak, nn * SLAB_BUILD_ROW, 6 * nn * 16)
+            else:
+                keep += nn * PACKED_ROW
+                peak = max(peak, nn * CSR_ROW, 48 * nn * 16)
+        resident = keep + peak
     if req.kind == "ed":
-        work = 3 * 48 * ni * 16
+        work = 2 * (ED_BASIS + 8) * ni * 16
     elif req.kind == "xas":
-        work = 4 * nn * 16 * max(req.ngs, 1)
+        work = 6 * nn * 16 * max(req.ngs, 1)
     else:
-        n_om = len(req.omegas)
-        k = len(set(p for p in req.pols)) * req.ngs
-        K = len(req.pols) * req.ngs * n_om
-        work = (2 * k * req.linsys_max * ni + 4 * nn * k + 4 * ni * K) * 16
+        k, npout, K = _rixs_shape(req)
+        ops = (npout * ni * 30 + 2 * nn * 5) * 20  # D_out (and a relabelled copy), D_in
+        hn_phase = 6 * nn * k + K * ni
+        if rixs_streamed(req, budget):
+            hn_phase += STREAM_WINDOW * npout * k * ni
+        else:
+            hn_phase += npout * k * req.linsys_max * ni
+        final_phase = K * ni + 4 * ni * min(K, FINAL_BLOCK)
+        work = ops + max(hn_phase, final_phase) * 16
     return int(resident + work)
 
 
@@ -225,7 +297,7 @@ class Server:
     def submit(self, req: Request) -> Future:
         fut = Future()
         req.t_submit = time.perf_counter()
-        if estimate_bytes(req, False) > self.budget:
+        if estimate_bytes(req, False, self.budget) > self.budget:
             fut.set_exception(MemoryError(f"request {req.id} needs more than the HBM budget"))
             return fut
         with self.cv:
@@ -284,7 +356,7 @@ class Server:
                 picked = None
                 for i, (req, fut) in enumerate(self.waiting):
                     cached = req.model in self.residents
-                    need = estimate_bytes(req, cached)
+                    need = estimate_bytes(req, cached, self.budget)
                     if self._resident_bytes() + self.inflight_bytes + need > self.budget:
                         self._evict_for(need)
                     if self._resident_bytes() + self.inflight_bytes + need <= self.budget:
@@ -307,7 +379,7 @@ class Server:
                 if not group:
                     continue
                 req = group[0][0]
-                need = sum(estimate_bytes(r, r.model in self.residents) for r, _ in group)
+                need = sum(estimate_bytes(r, r.model in self.residents, self.budget) for r, _ in group)
                 res = self._resident(req.model)
                 res.busy += 1
                 self.inflight_bytes += need
@@ -363,16 +435,20 @@ class Server:
         allw = np.unique(np.concatenate(oms))
         pins = sorted(set(siam_pol_in(p) for r, _ in group for p in r.pols))
         pouts = sorted(set(siam_pol_out(p) for r, _ in group for p in r.pols))
+        forms = {}
+        for key, M in (("hf", res.Hi), ("hn", res.Hn)):
+            if isinstance(M, device.PackedMatrix):
+                forms.setdefault("packed", {})[key] = M
+            elif isinstance(M, device.KronMatrix):
+                forms.setdefault("kron", {})[key] = M
         P = rixs.RixsProblem(Hn=res.Hn, Hf=res.Hi, Din=[res.op("in", p) for p in pins],
                              Dout=[res.op("out", p) for p in pouts], gs_e=gs_e[:G],
-                             gs_v=gs_v[:, :G].contiguous(),
-                             packed={k: v for k, v in (("hf", res.packed.get("hi")), ("hn", res.packed.get("hn")))
-                                     if v is not None},
-                             kron={k: v for k, v in (("hf", res.kron.get("hi")), ("hn", res.kron.get("hn")))
-                                   if v is not None})
+                             gs_v=gs_v[:, :G].contiguous(), **forms)
+        widest = max((r for r, _ in group), key=lambda r: _rixs_shape(r)[0])
         out = rixs.rixs_spectra(P, allw, req.gamma_c, req.eloss, req.gamma_f, nkryl=req.nkryl,
                                 linsys_tol=req.linsys_tol, linsys_max=req.linsys_max, temperature=req.temperature,
-                                per_gs=True)
+                                per_gs=True, stream=rixs_streamed(widest, self.budget), stream_window=STREAM_WINDOW,
+                                final_block=FINAL_BLOCK)
         results = []
         for (r, _), om in zip(group, oms):
             idx = np.searchsorted(allw, om)
@@ -394,11 +470,10 @@ class Server:
             spans.append((c0, c0 + r.ngs))
             c0 += r.ngs
         phi = torch.cat(phis, dim=1).contiguous()
-        kn, pk = res.kron.get("hn"), res.packed.get("hn")
-        if kn is not None:  # the slab product, on start vectors in its row order
-            kr = device.krylov(kn, kn.to_slab(phi), group[0][0].nkryl)
+        if isinstance(res.Hn, device.KronMatrix):  # the slab product, on start vectors in its row order
+            kr = device.krylov(res.Hn, res.Hn.to_slab(phi), group[0][0].nkryl)
         else:
-            kr = device.krylov(res.Hn, phi, group[0][0].nkryl, apply=dict(packed=pk) if pk is not None else None)
+            kr = device.krylov(res.Hn, phi, group[0][0].nkryl)
         norm = kr.norm.cpu().numpy()
         out = []
         for (r, _), (a, b) in zip(group, spans):

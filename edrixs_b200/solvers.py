@@ -73,8 +73,10 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
                 c64=False, verbose=False, packed=None):
     """Lowest `nev` eigenvalues (ascending) and `nvec` eigenvectors (n, nvec) of Hermitian H.
     packed: the packed form of H (device.pack); the block products then run on it.  H itself
-    may be a PackedMatrix when its CSR is no longer held."""
-    if isinstance(H, device.PackedMatrix):
+    may be a PackedMatrix when its CSR is no longer held, or a KronMatrix (the products run in
+    its slab order; the eigenvectors are returned in the reference's row order)."""
+    slab = isinstance(H, device.KronMatrix)
+    if slab or isinstance(H, device.PackedMatrix):
         packed = H
     n = H.nrows
     nvec = nev if nvec is None else nvec
@@ -85,7 +87,7 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
         mmax = max(3 * want + 4 * b, 40)
     mmax = ((mmax + b - 1) // b) * b
     if n <= max(mmax + b, 64):
-        if isinstance(H, device.PackedMatrix):
+        if not isinstance(H, device.CSR):
             raise ValueError("lowest_eigs: the dense solver of a small matrix needs its CSR")
         return dense_eigs(H, nev)[0], dense_eigs(H, nvec)[1]
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -121,8 +123,10 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
         theta, Y = np.linalg.eigh(Th)
         Bl = T[m:m + b, m - b:m]
         res = np.linalg.norm(Bl @ Y[m - b:m, :], axis=0)
-        # off-block-tridiagonal leakage after restarts is covered by using the full T
-        conv = res[:want] <= tol * max(1.0, 1.0)
+        # off-block-tridiagonal leakage after restarts is covered by using the full T.
+        # Converged: residual <= tol x |Ritz value| (ARPACK's test, which this solver replaces
+        # for ed_solver = 2), with |Ritz value| floored at 1
+        conv = res[:want] <= tol * np.maximum(1.0, np.abs(theta[:want]))
         if verbose:
             print(f"restart {restart}: theta={theta[:want]} res={res[:want]}")
         if np.all(conv):
@@ -147,7 +151,7 @@ def lowest_eigs(H: device.CSR, nev, nvec=None, tol=1e-9, block=None, mmax=None, 
     Yv = torch.from_numpy(Y[:, :nvec].copy()).to(dev)
     U = (Yv.T @ V[:m]).T.contiguous()          # n x nvec
     U = U / torch.linalg.vector_norm(U, dim=0, keepdim=True)
-    return theta[:nev].copy(), U
+    return theta[:nev].copy(), (H.from_slab(U).contiguous() if slab else U)
 
 
 def _plain_replay(a, b, neff, computed, nev, max_niter, eval_tol):

@@ -86,3 +86,30 @@ def test_failed_request_does_not_stop_server(cuda):
         assert len(ok["eigvals"]) == 2
     finally:
         srv.shutdown()
+
+
+def test_slab_only_residents_match_packed(cuda, monkeypatch):
+    """Intermediate sectors above serve.SLAB_ONLY_ROWS are held in the slab form alone (no CSR
+    built), with the absorption edge from a plain Lanczos run.  With the threshold at 0 the
+    same XAS and RIXS requests give the results of the packed residents within 1e-6."""
+    from edrixs_b200 import device, serve
+    from edrixs_b200.serve import ModelSpec, Request, Server
+    m = ModelSpec(4, 5, 31)
+    eloss = np.linspace(-0.5, 8.0, 300)
+    reqs = [lambda: Request("rixs", m, ngs=2, omegas=np.array([0.5, 2.5]), eloss=eloss, gamma_c=0.6, gamma_f=0.1,
+                            pols=(0, 3), nkryl=60),
+            lambda: Request("xas", m, ngs=2, eloss=np.linspace(-3, 12, 300), gamma_c=0.3, pols=(1,), nkryl=80)]
+    out = {}
+    for thr in (serve.SLAB_ONLY_ROWS, 0):
+        monkeypatch.setattr(serve, "SLAB_ONLY_ROWS", thr)
+        srv = Server(hbm_budget=40e9, workers=1).start()
+        try:
+            out[thr] = [srv.submit(f()).result(timeout=600) for f in reqs]
+            Hn = srv.residents[m].Hn
+        finally:
+            srv.shutdown()
+        assert isinstance(Hn, device.KronMatrix if thr == 0 else device.PackedMatrix)
+    a, b = out[serve.SLAB_ONLY_ROWS], out[0]
+    assert rel_linf(b[0]["spectra"], a[0]["spectra"]) < 1e-6
+    assert rel_linf(b[1]["spectrum"], a[1]["spectrum"]) < 1e-6
+

@@ -40,6 +40,24 @@ def test_slab_product_equals_csr(nbath, N, mode):
     assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
 
 
+@pytest.mark.parametrize("nbath,N,mode", [(4, 5, "ham_n"), (6, 7, "ham_i"), (12, 3, "ham_n")])
+def test_permutation_from_a_basis_tensor_equals_host(nbath, N, mode):
+    """The row permutation computed with torch from a basis tensor (as the device path does,
+    here on the CPU) equals the numpy one."""
+    import torch
+    from edrixs_b200 import kron
+    m, t = _terms(nbath, N, seed=5)
+    nv = m.nv
+    sfx = "i" if mode == "ham_i" else "n"
+    basis = orc.fock_full_N(nv, N if mode == "ham_i" else N + 1)
+    kw = dict(num_val_orbs=nv, num_core_orbs=0 if mode == "ham_i" else 6)
+    a = kron.kron_spec(t["hop_" + sfx], t["coul_" + sfx], basis, mode, **kw)
+    b = kron.kron_spec(t["hop_" + sfx], t["coul_" + sfx], torch.from_numpy(np.asarray(basis, dtype=np.int64)), mode,
+                       **kw)
+    assert a is not None and b is not None and isinstance(b.perm, torch.Tensor)
+    assert np.array_equal(a.perm, b.perm.numpy())
+
+
 def test_no_slab_form_without_a_bath():
     """Two-body terms on every orbital (no bath): no slab form, the CSR products are used."""
     from edrixs_b200 import kron

@@ -9,7 +9,7 @@ import pytest
 def test_serve_mix_is_seeded_and_in_range():
     import bench
     from edrixs_b200 import siam
-    args = types.SimpleNamespace(serve_seed=7, serve_requests=48, serve_rate=50.0)
+    args = types.SimpleNamespace(serve_seed=7, serve_requests=48, serve_rate=50.0, serve_norb_max=26)
     a, b = bench.serve_mix(args), bench.serve_mix(args)
     assert [(t, r.kind, r.model) for t, r in a] == [(t, r.kind, r.model) for t, r in b]
     times = np.array([t for t, _ in a])
@@ -17,15 +17,19 @@ def test_serve_mix_is_seeded_and_in_range():
     npol_xas = len(siam.atomic()["xas_polvec"])
     for _, r in a:
         norb = 10 + r.model.nbath
-        assert 16 <= norb <= 22 and abs(r.model.nelec - norb // 2) <= 1
+        assert 16 <= norb <= 26 and abs(r.model.nelec - norb // 2) <= 1
         assert r.kind in ("ed", "xas", "rixs")
         if r.kind == "xas":
             assert 0 <= r.pols[0] < npol_xas
         if r.kind == "rixs":
             assert all(0 <= p < 4 for p in r.pols) and len(r.omegas) == 8
-        assert math.comb(norb, r.model.nelec) <= 705432
+        assert math.comb(norb, r.model.nelec) <= 10400600
     kinds = {r.kind for _, r in a}
     assert kinds == {"ed", "xas", "rixs"}
+    assert {10 + r.model.nbath for _, r in a} >= {16, 26}  # both ends of the stated range
+    small = bench.serve_mix(types.SimpleNamespace(serve_seed=7, serve_requests=48, serve_rate=50.0,
+                                                  serve_norb_max=22))
+    assert max(10 + r.model.nbath for _, r in small) <= 22
 
 
 def test_coalesce_key_groups_compatible_requests():
@@ -216,3 +220,20 @@ def test_shutdown_between_pick_and_queue_leaves_no_future_pending():
     worker.join(timeout=5)
     assert not worker.is_alive() and srv.stop_flag
     assert srv.free_workers == 1 and srv.inflight_bytes == 0
+
+
+def test_admission_estimate_of_large_models():
+    """The admission estimate of the largest models of the serving mix (26 valence
+    spin-orbitals) fits the 150 GB budget for ED, XAS and RIXS (slab-only H_n, streamed RIXS),
+    and keeps the stored-projection form for small RIXS requests."""
+    from edrixs_b200 import serve
+    from edrixs_b200.serve import ModelSpec, Request
+    big = ModelSpec(16, 13, 1)
+    eloss = np.linspace(-0.5, 12.0, 1000)
+    reqs = [Request("ed", big, ngs=4), Request("xas", big, ngs=3, eloss=eloss, pols=(0,)),
+            Request("rixs", big, ngs=3, omegas=np.linspace(0, 8, 8), eloss=eloss, pols=(0, 1, 2, 3))]
+    for r in reqs:
+        assert serve.estimate_bytes(r, False, 150e9) < 150e9, r.kind
+    assert serve.rixs_streamed(reqs[2], 150e9)
+    small = Request("rixs", ModelSpec(6, 8, 1), ngs=1, omegas=np.linspace(0, 8, 8), eloss=eloss, pols=(0,))
+    assert not serve.rixs_streamed(small, 150e9)

@@ -1051,7 +1051,11 @@ def run_serve(args):
         rk = [r for r in recs if r["kind"] == kind]
         lk = np.array([r["latency_s"] for r in rk]) * 1e3
         sk = np.array([r["service_s"] for r in rk]) * 1e3
-        by_kind[kind] = {"n": len(rk), "p50_ms": pct(lk, 50), "p99_ms": pct(lk, 99), "service_p50_ms": pct(sk, 50)}
+        by_norb = {}
+        for r in rk:
+            by_norb.setdefault(r["norb"], []).append(r["service_s"] * 1e3)
+        by_kind[kind] = {"n": len(rk), "p50_ms": pct(lk, 50), "p99_ms": pct(lk, 99), "service_p50_ms": pct(sk, 50),
+                         "service_max_ms_by_norb": {str(n): round(max(v), 1) for n, v in sorted(by_norb.items())}}
     dims = [math.comb(10 + r.model.nbath, r.model.nelec) for _, r in jobs]
     dims_n = [6 * math.comb(10 + r.model.nbath, r.model.nelec + 1) for _, r in jobs if r.kind != "ed"]
     line = {"metric": "serving mix: completed requests/s & p50/p99 latency (queueing + service)",

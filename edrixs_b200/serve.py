@@ -404,7 +404,8 @@ class Server:
                 for (req, fut), out in zip(group, outs):
                     req.t_start, req.t_done = t0, t1
                     self.records.append({"id": req.id, "kind": req.kind, "latency_s": t1 - req.t_submit,
-                                         "service_s": t1 - t0, "coalesced": len(group)})
+                                         "service_s": t1 - t0, "coalesced": len(group),
+                                         "norb": req.model.nv, "dims": _dims(req.model)})
                     fut.set_result(out)
             except Exception as e:  # a failed job fails its requests, never the server
                 for req, fut in group:

@@ -105,9 +105,10 @@ def kernel_case(args):
 def kernel_case_kron(args):
     """The apply kernels of this workload side by side, for a profiler: the packed product on
     H_f (256 final-state columns at the autotuner's usual shape; the vectors, 0.76 GB, exceed
-    L2), and on H_n (6 seed columns, one row per lane group) next to the slab product on H_n.
-    Every product runs one warm-up step first, then one step each in the order packed H_f,
-    slab H_n, packed H_n (launches 4-6 of k_lanczos_apply*)."""
+    L2), and on H_n (6 seed columns, one row per lane group) next to the two slab products on
+    H_n (staged and gather).  Every product runs one warm-up step first, then one step each in
+    the order packed H_f, staged slab H_n, packed H_n, gather slab H_n (launches 5-8 of
+    k_lanczos_apply*)."""
     import torch
     from edrixs_b200 import device
     m, t = workload_terms(args.nbath, args.nelec)
@@ -127,7 +128,8 @@ def kernel_case_kron(args):
     Vs = Kn.to_slab(V)
     hf = dict(col_group=32, tiles=2, threads=1024, blocks_per_sm=1, chunked=0)
     hn = dict(col_group=6, threads=1024, blocks_per_sm=1, rowslot=1)
-    runs = [(Pf, W, hf), (Kn, Vs, None), (Pn, V, hn)]
+    runs = [(Pf, W, hf), (Kn, Vs, dict(col_group=device.KRON_STAGED)), (Pn, V, hn),
+            (Kn, Vs, dict(col_group=device.KRON_GATHER, threads=256, blocks_per_sm=4))]
     for _ in range(2):  # a warm-up step of each, then the profiled one
         for A, X, ap in runs:
             device.krylov(A, X, 1, apply=ap)
@@ -657,7 +659,9 @@ def run_ours(args):
 
     def kname(packed, kron, cfg):
         if kron:
-            return "k_lanczos_apply_kron"
+            from edrixs_b200 import device
+            gather = bool(cfg and cfg.get("col_group") == device.KRON_GATHER)
+            return "k_lanczos_apply_kron_gather" if gather else "k_lanczos_apply_kron"
         rs = bool(cfg and cfg.get("rowslot"))
         return ("k_lanczos_apply_packed" if packed else "k_lanczos_apply") + ("_rs" if rs else "")
 
@@ -849,7 +853,9 @@ def run_scale(args):
       4. RIXS with complex64 H_n products on a subset of the incident energies;
       5. H_n rebuilt and packed (wide form), XAS on it, and the full 32-omega_in RIXS on the
          packed forms (two-pass streaming of D_out^+ v_i: storing it for every v_i would
-         take terabytes).
+         take terabytes);
+      6. H_n built in the slab form alone (no CSR), XAS and the full RIXS with its gather
+         product.
     Errors: XAS spectra (1000 points, Gamma = 0.3) of the complex64 and packed products
     against the FP64 CSR products; RIXS spectra with complex64 H_n products against the
     packed FP64 ones on the shared incident energies."""
@@ -1007,6 +1013,34 @@ def run_scale(args):
                    "c64_vs_packed_fp64_rel_linf": rel(rb.spectra, rc.spectra[sub]),
                    "c64_subset_omega_in": len(sub),
                    "hn_apply_ms_total": rc.stats.get("hn_apply_ms"), "hf_apply_ms_total": rc.stats.get("hf_apply_ms")}
+    # 6. H_n in the slab form, built without any CSR: XAS and the full RIXS request with its
+    # gather product (H_f stays packed)
+    del P, Pn
+    free()
+    t0 = tick()
+    Kn = device.kron_form(device.HAM_N, bn, t["hop_n"], t["coul_n"], num_val_orbs=nv, num_core_orbs=6)
+    tm["hn_slab_build_s"] = tick() - t0
+    if Kn is not None:
+        res["H_n"].update(slab_gb=gb(Kn.nbytes()), slab_max_rows=Kn.max_rows, slabs=Kn.spec.nslab)
+        cfg_k = dict(col_group=device.KRON_GATHER)
+        t0 = tick()
+        xk = device.krylov(Kn, Kn.to_slab(seeds), nk, timing=True, apply=cfg_k)
+        tm["xas_slab_s"] = tick() - t0
+        tm["xas_slab_apply_ms_per_step"] = xk.apply_ms / max(xk.apply_launches, 1)
+        res["xas"]["slab_vs_fp64_rel_linf"] = rel(xas_spec(xk), sa)
+        del xk
+        P = rixs.RixsProblem(Hn=Kn, Hf=Pi, Din=[], Dout=Dout, gs_e=np.asarray(gs_e), gs_v=gs_v)
+        P.kron["hn"] = Kn
+        P.packed["hf"] = Pi
+        P.meta[("apply", "hn", seeds.shape[1], False)] = dict(cfg_k, kron=1)
+        P.meta[("apply", "hf", 128, False)] = hf_cfg
+        t0 = tick()
+        rk = rixs.rixs_spectra(P, omegas, 0.6, eloss, 0.1, seeds=seeds, final_block=128, **kw)
+        tm["rixs_slab_s"] = tick() - t0
+        res["rixs"].update(slab_points_per_s=round(npts / tm["rixs_slab_s"], 3),
+                           slab_vs_packed_rel_linf=rel(rk.spectra, rc.spectra),
+                           slab_minres_iters_equal=bool(np.array_equal(rk.iters, rc.iters)),
+                           slab_hn_apply_ms_total=rk.stats.get("hn_apply_ms"))
     res["times_s"] = {k: round(v, 3) for k, v in tm.items()}
     res["peak_device_gb"] = gb(torch.cuda.max_memory_allocated())
     print(json.dumps(res), flush=True)

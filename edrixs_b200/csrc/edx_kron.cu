@@ -387,8 +387,24 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron(KronView K, const 
 // row outside its slab (an inconsistent slab form) is skipped and reported (err = 2).
 constexpr int KG_HOPS = 2;  // hops whose source rows load together
 
+// KC complex values of one row tile: 32-byte loads (two complex values each) when the tile
+// starts on a 32-byte boundary and is full (even k, even KC), else 16-byte loads
+__device__ __forceinline__ void ld_c2(const double2* p, double2& a, double2& b) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(p));
+}
+template <int KC>
+__device__ __forceinline__ void ld_tile(const double2* p, int kc, bool pairs, double2* xs) {
+    if (KC % 2 == 0 && pairs) {
+#pragma unroll
+        for (int h = 0; h < KC / 2; ++h) ld_c2(p + 2 * h, xs[2 * h], xs[2 * h + 1]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < KC; ++j) xs[j] = j < kc ? ldx(p + j) : make_double2(0.0, 0.0);
+    }
+}
+
 template <int KC, bool LANCZOS>
-__global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron_gather(KronView K, int64_t nrows,
+__global__ void __launch_bounds__(KR_NT, 2) k_lanczos_apply_kron_gather(KronView K, int64_t nrows,
                                                                      const double2* __restrict__ X,
                                                                      double2* __restrict__ Y, KrylovState S, int k,
                                                                      int it, unsigned* __restrict__ tile_ticket,
@@ -417,6 +433,7 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron_gather(KronView K,
         }
     }
     const uint32_t full = (1u << K.nb) - 1u;
+    const bool pairs = (k % 2 == 0) && kc == KC;  // every row tile of this block is 32-byte aligned
     bool bad = false;
     for (int64_t i = (int64_t)blockIdx.x * KR_NT + tid; i < nrows; i += (int64_t)gridDim.x * KR_NT) {
         int lo = 0, hi = K.nslab - 1;  // the last slab with slab_off <= i
@@ -454,10 +471,8 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron_gather(KronView K,
                     v.x += d.x;
                     v.y += d.y;
                 }
-                const double2* xr = X + (int64_t)(soff + r) * k + c0;
                 double2 xs[KC];
-#pragma unroll
-                for (int j = 0; j < KC; ++j) xs[j] = j < kc ? ldx(xr + j) : make_double2(0.0, 0.0);
+                ld_tile<KC>(X + (int64_t)(soff + r) * k + c0, kc, pairs, xs);
 #pragma unroll
                 for (int j = 0; j < KC; ++j) acc[j] = fma_c(v, xs[j], acc[j]);
             } else {
@@ -493,10 +508,14 @@ __global__ void __launch_bounds__(KR_NT) k_lanczos_apply_kron_gather(KronView K,
                     }
                     double2 xs[KG_HOPS][KC];
 #pragma unroll
-                    for (int h = 0; h < KG_HOPS; ++h)
+                    for (int h = 0; h < KG_HOPS; ++h) {
+                        if (ok[h]) {
+                            ld_tile<KC>(X + row[h], kc, pairs, xs[h]);
+                        } else {
 #pragma unroll
-                        for (int j = 0; j < KC; ++j)
-                            xs[h][j] = (ok[h] && j < kc) ? ldx(X + row[h] + j) : make_double2(0.0, 0.0);
+                            for (int j = 0; j < KC; ++j) xs[h][j] = make_double2(0.0, 0.0);
+                        }
+                    }
 #pragma unroll
                     for (int h = 0; h < KG_HOPS; ++h)
 #pragma unroll
@@ -620,11 +639,12 @@ static bool gather_of(const edx_kron* K, int variant) { return variant == EDX_KR
 // columns per thread of the gather product: the smallest supported count >= k, 8 beyond
 static int gather_kc(int k) { return kc_of(k); }
 
-int kron_grid_x(const edx_kron* K, int k, int variant) {
+int kron_grid_x(const edx_kron* K, int k, int variant, int blocks_per_sm) {
     if (gather_of(K, variant)) {
         const int kc = gather_kc(k);
         const int ntile = (k + kc - 1) / kc;
-        const int64_t target = (int64_t)num_sms() * 8 * 4;  // 8 blocks of 256 threads per SM, 4 rounds
+        // blocks_per_sm x SMs blocks in all (0: 8 blocks of 256 threads per SM, 4 rounds)
+        const int64_t target = (int64_t)num_sms() * (blocks_per_sm > 0 ? blocks_per_sm : 8 * 4);
         const int64_t gx = (target + ntile - 1) / ntile;
         const int64_t need = (K->nrows + KR_NT - 1) / KR_NT;
         return (int)std::max<int64_t>(1, std::min(gx, need));
@@ -673,7 +693,7 @@ static int launch_kron_rpt(const edx_kron* K, const CUtensorMap* tm, const doubl
     EDX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn));
     const int ntile = (k + KR_CW - 1) / KR_CW;
     EDX_REQUIRE(ntile <= 65535, "slab form: too many column tiles");
-    dim3 grid(kron_grid_x(K, k, 0), ntile);
+    dim3 grid(kron_grid_x(K, k, 0, 0), ntile);
     kern<<<grid, KR_NT, sm, st>>>(view_of(K), *tm, X, Y, S, k, it, stage_rows_of(K), tt, err);
     EDX_CHECK_LAUNCH();
     return EDX_OK;
@@ -693,12 +713,12 @@ static int launch_kron_kc(const edx_kron* K, const CUtensorMap* tm, const double
 
 template <int KC, bool LANCZOS>
 static int launch_gather_kc(const edx_kron* K, const double2* X, double2* Y, const KrylovState& S, int k, int it,
-                            unsigned* tt, int* err, cudaStream_t st) {
+                            unsigned* tt, int* err, int bps, cudaStream_t st) {
     auto kern = k_lanczos_apply_kron_gather<KC, LANCZOS>;
     const size_t sm = 2 * (size_t)K->nah * K->nb * sizeof(double2);
     const int ntile = (k + KC - 1) / KC;
     EDX_REQUIRE(ntile <= 65535, "slab form: too many column tiles");
-    dim3 grid(kron_grid_x(K, k, EDX_KRON_GATHER), ntile);
+    dim3 grid(kron_grid_x(K, k, EDX_KRON_GATHER, bps), ntile);
     kern<<<grid, KR_NT, sm, st>>>(view_of(K), K->nrows, X, Y, S, k, it, tt, err);
     EDX_CHECK_LAUNCH();
     return EDX_OK;
@@ -706,17 +726,17 @@ static int launch_gather_kc(const edx_kron* K, const double2* X, double2* Y, con
 
 template <bool LANCZOS>
 static int launch_kron(const edx_kron* K, const CUtensorMap* tm, const double2* X, double2* Y, const KrylovState& S,
-                       int k, int it, unsigned* tt, int* err, int variant, cudaStream_t st) {
+                       int k, int it, unsigned* tt, int* err, int variant, int bps, cudaStream_t st) {
     if (variant == EDX_KRON_STAGED && !staged_fits(K))
         return fail(EDX_ERR_INVALID, "slab form: slabs of %d rows do not fit the staged product's shared memory",
                     K->max_rows);
     if (gather_of(K, variant)) {
         switch (gather_kc(k)) {
-        case 1: return launch_gather_kc<1, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
-        case 2: return launch_gather_kc<2, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
-        case 4: return launch_gather_kc<4, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
-        case 6: return launch_gather_kc<6, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
-        default: return launch_gather_kc<8, LANCZOS>(K, X, Y, S, k, it, tt, err, st);
+        case 1: return launch_gather_kc<1, LANCZOS>(K, X, Y, S, k, it, tt, err, bps, st);
+        case 2: return launch_gather_kc<2, LANCZOS>(K, X, Y, S, k, it, tt, err, bps, st);
+        case 4: return launch_gather_kc<4, LANCZOS>(K, X, Y, S, k, it, tt, err, bps, st);
+        case 6: return launch_gather_kc<6, LANCZOS>(K, X, Y, S, k, it, tt, err, bps, st);
+        default: return launch_gather_kc<8, LANCZOS>(K, X, Y, S, k, it, tt, err, bps, st);
         }
     }
     switch (kc_of(k)) {
@@ -735,9 +755,9 @@ int kron_col_group(int /*k*/, int requested) {
 }
 
 int apply_kron(const edx_kron* K, const void* tmap, const double2* Vc, double2* Vp, const KrylovState& S, int it,
-               unsigned* tile_ticket, int* err, int col_group, cudaStream_t st) {
+               unsigned* tile_ticket, int* err, int col_group, int blocks_per_sm, cudaStream_t st) {
     return launch_kron<true>(K, static_cast<const CUtensorMap*>(tmap), Vc, Vp, S, S.k, it, tile_ticket, err,
-                             kron_col_group(S.k, col_group), st);
+                             kron_col_group(S.k, col_group), blocks_per_sm, st);
 }
 
 __global__ void k_permute_rows(int64_t n, int k, const double2* __restrict__ src, int64_t lds,
@@ -776,7 +796,7 @@ extern "C" int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double
         return rc;
     KrylovState S{};
     rc = launch_kron<false>(K, &tm, reinterpret_cast<const double2*>(d_x), reinterpret_cast<double2*>(d_y), S, k, 0,
-                            nullptr, err, variant, st);
+                            nullptr, err, variant, 0, st);
     if (rc) return rc;
     int h = 0;
     EDX_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));

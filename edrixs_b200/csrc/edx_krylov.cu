@@ -843,7 +843,8 @@ extern "C" int edx_krylov_workspace(int64_t n, int k, const edx_krylov_opts* opt
     if (opts && opts->apply_kron) {
         int rc = kron_check(opts->apply_kron);
         if (rc) return rc;
-        gx = std::max(gx, kron_grid_x(opts->apply_kron, k, kron_col_group(k, opts->apply_col_group)));
+        gx = std::max(gx, kron_grid_x(opts->apply_kron, k, kron_col_group(k, opts->apply_col_group),
+                                      opts->apply_blocks_per_sm));
     }
     krylov_layout(s, n, k, opts ? opts->nshift : 0, maxn, gx, nullptr);
     *bytes = s.s.bytes();
@@ -918,7 +919,7 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
     const int kw = pow2_kw(k);  // layout of the element-wise recurrence kernels
     const int gy = (k + kw - 1) / kw;
     int gx = num_sms() * 8;
-    if (kron) gx = std::max(gx, kron_grid_x(kron, k, kron_cw));
+    if (kron) gx = std::max(gx, kron_grid_x(kron, k, kron_cw, opts->apply_blocks_per_sm));
     Workspace w(d_work, work_bytes);
     KrylovWs ws;
     krylov_layout(w, n, k, nshift, maxn, gx, &ws);
@@ -1032,7 +1033,7 @@ extern "C" int edx_krylov(const edx_csr* A, int k, const double* d_v0, int maxn,
         }
         if (kron)
             rc = apply_kron(kron, Vc == ws.Vc ? static_cast<const void*>(&tm_c) : static_cast<const void*>(&tm_p), Vc,
-                            Vp, S, it, ws.kticket, ws.kron_err, kron_cw, st);
+                            Vp, S, it, ws.kticket, ws.kron_err, kron_cw, opts->apply_blocks_per_sm, st);
         else if (packed)
             rc = apply_packed(packed, Vc, Vp, S, it, cfg, st);
         else

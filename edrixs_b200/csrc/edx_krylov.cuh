@@ -44,10 +44,10 @@ struct KrylovState {
 };
 
 int apply_kron(const edx_kron* K, const void* tmap, const double2* Vc, double2* Vp, const KrylovState& S, int it,
-               unsigned* tile_ticket, int* err, int col_group, cudaStream_t st);
+               unsigned* tile_ticket, int* err, int col_group, int blocks_per_sm, cudaStream_t st);
 int kron_tensor_map(const edx_kron* K, const double2* X, int k, int col_group, void* tmap_out);
 int kron_check(const edx_kron* K);
-int kron_grid_x(const edx_kron* K, int k, int col_group);
+int kron_grid_x(const edx_kron* K, int k, int col_group, int blocks_per_sm);
 int kron_col_group(int k, int requested);
 
 }  // namespace edx

@@ -81,7 +81,7 @@ def _apply_args(cfg, packed, c64, kron=None):
         if cfg.get("kron"):
             if kron is None:
                 raise ValueError("the tuned launch shape needs the slab form")
-            return dict(col_group=cfg.get("col_group", 0), kron=kron)
+            return dict({x: v for x, v in cfg.items() if x in ("col_group", "threads", "blocks_per_sm")}, kron=kron)
         if cfg.get("packed"):
             if packed is None:
                 raise ValueError("the tuned launch shape needs the packed form")

@@ -166,7 +166,7 @@ def kernel_case_all(args):
     (768 pole sets x 2000 points), the density matrix, the packed SpMM (narrow and wide
     forms), the Gram-Schmidt and CholeskyQR passes of the eigensolver, the few-column Lanczos
     products with one row per lane group, 16 Lanczos steps with streamed projections, and the
-    slab form of H_n (product, Lanczos step, row permutations)."""
+    slab form of H_n (product and Lanczos step in both variants, row permutations)."""
     import torch
     from edrixs_b200 import device
     m, t = workload_terms(args.nbath, args.nelec)
@@ -229,6 +229,8 @@ def kernel_case_all(args):
     Vs = Kn.to_slab(V)
     device.spmm(Kn, Vs)
     device.krylov(Kn, Vs, 2)
+    device.spmm(Kn, Vs, col_group=device.KRON_GATHER)
+    device.krylov(Kn, Vs, 2, apply=dict(col_group=device.KRON_GATHER, threads=256, blocks_per_sm=4))
     Kn.from_slab(Vs)
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": "all", "nnz_Hn": Hn.nnz, "nnz_Hf": Hf.nnz, "nnz_Din": Din.nnz,

@@ -99,6 +99,8 @@ _SIGS = {
     "edx_kron_spmm": (ctypes.c_int, [ctypes.POINTER(Kron), ctypes.c_int, vp, vp, ctypes.c_int, vp, ctypes.c_size_t,
                                      vp]),
     "edx_permute_rows": (ctypes.c_int, [i64, ctypes.c_int, vp, i64, vp, vp, i64, vp]),
+    "edx_proj_combine": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        i64, vp, i64, ctypes.c_int, vp, i64, vp]),
     "edx_gs_workspace": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "edx_gs_dot": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp, ctypes.c_size_t, vp]),
     "edx_gs_update": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, vp, ctypes.c_int, vp, vp]),

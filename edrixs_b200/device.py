@@ -417,6 +417,29 @@ def permute_rows(X, idx):
     return Y.reshape(-1) if X.dim() == 1 else Y
 
 
+def proj_combine(projs, y, k, nw, m):
+    """Final-state start vectors from stored projections (edx_proj_combine): returns the
+    row-major (nrows, len(projs) * k * nw) block with column (p * k + c) * nw + w equal to
+    sum_{i < m} y[c * nw + w, i] * projs[p][c, i, :].  projs: (k, steps, nrows) complex128
+    blocks with rows contiguous, such as krylov's stored projections (views of (k, maxn,
+    nrows) buffers); y: (k * nw, ldy) complex128 with ldy >= m."""
+    np_ = len(projs)
+    kk, steps, nrows = projs[0].shape
+    if kk != k or y.shape[0] != k * nw or y.stride(1) != 1 or y.dtype != torch.complex128 or m > steps:
+        raise ValueError("proj_combine: shapes or layout do not match")
+    cstride = projs[0].stride(0)
+    for P in projs:
+        if (tuple(P.shape) != (k, steps, nrows) or P.stride(2) != 1 or P.stride(1) != nrows or P.stride(0) != cstride
+                or cstride % nrows or P.dtype != torch.complex128):
+            raise ValueError("proj_combine: projections must be (k, steps, nrows) complex128 blocks of contiguous "
+                             "rows with one column stride")
+    out = torch.empty((nrows, np_ * k * nw), dtype=torch.complex128, device=y.device)
+    ptrs = (ctypes.c_void_p * np_)(*[P.data_ptr() for P in projs])
+    call("edx_proj_combine", np_, ptrs, k, cstride // nrows, int(m), nrows, _ptr(y), y.stride(0), nw, _ptr(out),
+         out.stride(0), _stream())
+    return out
+
+
 def spmm(A, X, Y=None, alpha=1.0, sigma=0.0, beta=0.0, c64=False, col_group=0):
     """Y = alpha*(A X) + sigma*X + beta*Y; X is (ncols,) or (ncols, k) row-major.  A is a CSR
     or a PackedMatrix (edx_spmm_packed)."""

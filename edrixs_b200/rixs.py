@@ -184,16 +184,10 @@ def rixs_spectra(P: RixsProblem, omegas, gamma_c, eloss, gamma_f, *, nkryl=150, 
                  launches=npin + 4 + npout + it_n * (3 + 2 * npout) + (Kn is not None) + (Kf is not None),
                  streamed=bool(stream))
     if not stream:
-        Y = r.shift_y.view(k, n_om, -1)[:, :, :m]                 # (k, n_om, m)
-        # phi[p_out][c, w, :] = sum_i Y[c, w, i] * (D_out^+ v_i)[:]
-        phis = []
-        for po in range(npout):
-            W = r.proj[po][:, :m, :]                               # (k, m, n_f)
-            phis.append(torch.matmul(Y, W))                        # (k, n_om, n_f)
+        # V0[:, (p_out * k + c) * n_om + w] = sum_{i < m} Y[c, w, i] * (D_out(p_out)^+ v_i)[c]
+        V0 = device.proj_combine(r.proj, r.shift_y, k, n_om, m)   # (n_f, K) row-major
+        stats["launches"] += npout * k
         del r
-        Phi = torch.stack(phis, dim=0)                             # (npout, k, n_om, n_f)
-        V0 = Phi.reshape(K, nf).T.contiguous()                     # (n_f, K) row-major
-        del Phi, phis
     else:
         # pass 2: the same m Lanczos vectors again (deterministic reductions: the same
         # vectors), each D_out^+ v_i folded into phi as it appears, B vectors at a time

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define EDX_ABI_VERSION 6
+#define EDX_ABI_VERSION 7
 
 /* status codes */
 #define EDX_OK 0
@@ -365,6 +365,16 @@ int edx_minres_workspace(int64_t n, size_t* bytes);
 int edx_minres(const edx_csr* A, double alpha_re, double alpha_im, double sigma_re,
                double sigma_im, const double* d_b, double* d_x, double tol, int maxit,
                int* iters_out, double* res_out, void* d_work, size_t work_bytes, void* stream);
+
+/* Final-state start vectors of the batched RIXS from stored projections (the D_out^+ x of
+ * src/rixs_driver.f90 for every shift, after edx_krylov with stored proj_out):
+ *   d_out[r*ld_out + (p*k + c)*nw + w] = sum_{i<m} y[(c*nw + w)*ldy + i] * proj_p[(c*maxn + i)*nrows + r]
+ * for p < np, c < k, w < nw, r < nrows (complex128): proj_p = d_proj[p] (host array of np
+ * device pointers, the [k][maxn][nrows] blocks edx_krylov writes), y the shifts' MINRES
+ * coefficients in the Lanczos basis (shift_y: column c's nw shifts, rows of length ldy >= m),
+ * m <= maxn the Lanczos vectors used.  Each output is one sum over i in order. */
+int edx_proj_combine(int np, const double* const* d_proj, int k, int maxn, int m, int64_t nrows,
+                     const double* d_y, int64_t ldy, int nw, double* d_out, int64_t ld_out, void* stream);
 
 /* Continued fraction of get_spectra_from_poles (edrixs/plot_spectrum.py:41-61) for nset
  * pole sets on one grid:  spec[w] (+)= sum_s weight[s] * norm[s] * (-1/pi) *

@@ -361,3 +361,26 @@ def test_krylov_zero_start_column(hn_pair):
     spec = device.cf_spectrum(r.neff, r.alpha, r.beta, np.zeros(3), r.norm.cpu().numpy(), np.ones(3),
                               np.linspace(-5, 5, 50), 0.3, per_set=True)
     assert torch.isfinite(spec).all() and spec[1].abs().max().item() == 0.0
+
+
+@pytest.mark.parametrize("nrows,k,maxn,m,nw,np_", [(1000, 3, 37, 29, 70, 2), (64, 1, 8, 8, 64, 1), (4097, 6, 50, 1, 5, 2)])
+def test_proj_combine_equals_matmul(cuda, nrows, k, maxn, m, nw, np_):
+    """edx_proj_combine (the batched RIXS's final-state start vectors from stored projections)
+    equals the product and transpose it replaces, for ragged tiles of rows, shifts and
+    Lanczos vectors."""
+    import torch
+    from edrixs_b200 import device
+    g = torch.Generator(device="cuda")
+    g.manual_seed(nrows + m)
+
+    def rnd(*shape):
+        return torch.complex(torch.randn(shape, dtype=torch.float64, device="cuda", generator=g),
+                             torch.randn(shape, dtype=torch.float64, device="cuda", generator=g))
+
+    projs = [rnd(k, maxn, nrows)[:, :m + (maxn - m) // 2, :] for _ in range(np_)]  # views, as krylov returns
+    y = rnd(k * nw, maxn)
+    got = device.proj_combine(projs, y, k, nw, m)
+    Y = y.view(k, nw, maxn)[:, :, :m]
+    want = torch.stack([torch.matmul(Y, P[:, :m, :]) for P in projs], dim=0).reshape(np_ * k * nw, nrows).T
+    assert got.shape == want.shape
+    assert float((got - want).abs().max()) <= 1e-13 * float(want.abs().max())

@@ -169,7 +169,7 @@ def test_library_exports_every_header_symbol():
         assert hasattr(L, n), n
     # the binding declares every header function and nothing else
     assert set(_lib.exported_symbols()) <= set(names)
-    assert L.edx_abi_version() == 6
+    assert L.edx_abi_version() == 7
 
 
 def test_abi_error_path_without_gpu():

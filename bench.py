@@ -717,7 +717,7 @@ def run_ours(args):
 
     if rank == 0:
         clocks = clk.summary()
-        if not args.no_other_configs:
+        if not args.no_other_configs and ws == 1:  # single-GPU figures: once, in the one-GPU run
             extra["other_configs"] = other_configs()
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,

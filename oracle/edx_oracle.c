@@ -2,8 +2,8 @@
  * edx_oracle.c -- CPU FP64 restatement of the EDRIXS Fortran hot path.
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle: it is compiled into
- * oracle/libedx_oracle.so and loaded by tests/, by __graft_entry__.smoke() as the
- * checker, and by bench.py's CPU-baseline leg.  The product path (edrixs_b200) never
+ * oracle/libedx_oracle.so and loaded by tests/, by __graft_entry__.smoke() to check its
+ * results, and by bench.py's CPU-baseline leg.  The product path (edrixs_b200) never
  * links or calls it.
  *
  * Every routine restates one reference routine (paths relative to the reference repo):

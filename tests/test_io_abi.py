@@ -278,7 +278,7 @@ def test_admission_estimates_and_oversize_rejection():
 
 def test_product_package_never_imports_the_oracle():
     """The oracle is test infrastructure: no module of the product package imports it, so no
-    product call can route through it (bench.py's CPU-baseline leg and smoke()'s checker are
+    product call can route through it (bench.py's CPU-baseline leg and smoke()'s result check are
     the only other importers)."""
     import ast
     pkg = os.path.join(ROOT, "edrixs_b200")

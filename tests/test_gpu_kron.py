@@ -189,3 +189,25 @@ def test_lowest_eigs_on_slab_form(cuda):
     assert np.all(ov > 1 - 1e-8) or np.abs(e[1] - e[0]) < 1e-8  # degenerate pairs may rotate
     ep, _ = solvers.plain_lanczos_eigs(K, 1, 0, 400, 1e-10)
     assert abs(ep[0] - e[0]) < 1e-9
+
+
+def test_understated_slab_size_is_reported_not_read_past(cuda):
+    """A slab form whose max_rows understates its largest slab: the staged product clamps the
+    staged boxes, the rows it holds and the hop ranks to its ring, and both the product and
+    the Lanczos step report EDX_ERR_INVALID (the kernel's own range checks)."""
+    import dataclasses
+    from edrixs_b200 import _lib, device
+    H, K = _both(10, 6, "ham_i")  # slabs of up to C(10, 5) = 252 rows
+    assert K.max_rows == 252
+    bad = dataclasses.replace(K, max_rows=K.max_rows // 2)
+    X = _rand(H.nrows, 8, 5)
+    with pytest.raises(_lib.EdxError) as e:
+        device.spmm(bad, bad.to_slab(X), col_group=device.KRON_STAGED)
+    assert e.value.code == 1
+    with pytest.raises(_lib.EdxError) as e:
+        device.krylov(bad, bad.to_slab(X), 4, apply=dict(col_group=device.KRON_STAGED))
+    assert e.value.code == 1
+    # the consistent form still works afterwards (the context is intact)
+    want = device.spmm(H, X)
+    got = K.from_slab(device.spmm(K, K.to_slab(X)))
+    assert float((got - want).abs().max()) <= 1e-13 * float(want.abs().max())

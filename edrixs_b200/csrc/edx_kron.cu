@@ -635,12 +635,17 @@ int kron_check(const edx_kron* K) {
 // the staged product needs every slab within one block (4 rows per thread at most) and the
 // ring of staged slabs within shared memory
 static bool staged_fits(const edx_kron* K) { return rpt_of(K) != 0 && smem_bytes(K) + 8 * 1024 <= 227 * 1024; }
-static bool gather_of(const edx_kron* K, int variant) { return variant == EDX_KRON_GATHER || !staged_fits(K); }
+// AUTO: the gather product for up to 8 columns (one tile: 0.70 against 0.89 ms on a 1 M-row
+// impurity H_n) and whenever the staged ring does not fit; the staged product for wider
+// blocks (96 columns: 2.1 against 2.9 ms; 768: 16.5 against 22.3 ms)
+static bool gather_of(const edx_kron* K, int variant, int k) {
+    return variant == EDX_KRON_GATHER || !staged_fits(K) || (variant != EDX_KRON_STAGED && k <= KR_CW);
+}
 // columns per thread of the gather product: the smallest supported count >= k, 8 beyond
 static int gather_kc(int k) { return kc_of(k); }
 
 int kron_grid_x(const edx_kron* K, int k, int variant, int blocks_per_sm) {
-    if (gather_of(K, variant)) {
+    if (gather_of(K, variant, k)) {
         const int kc = gather_kc(k);
         const int ntile = (k + kc - 1) / kc;
         // blocks_per_sm x SMs blocks in all (0: 8 blocks of 256 threads per SM, 4 rounds)
@@ -730,7 +735,7 @@ static int launch_kron(const edx_kron* K, const CUtensorMap* tm, const double2* 
     if (variant == EDX_KRON_STAGED && !staged_fits(K))
         return fail(EDX_ERR_INVALID, "slab form: slabs of %d rows do not fit the staged product's shared memory",
                     K->max_rows);
-    if (gather_of(K, variant)) {
+    if (gather_of(K, variant, k)) {
         switch (gather_kc(k)) {
         case 1: return launch_gather_kc<1, LANCZOS>(K, X, Y, S, k, it, tt, err, bps, st);
         case 2: return launch_gather_kc<2, LANCZOS>(K, X, Y, S, k, it, tt, err, bps, st);
@@ -792,7 +797,7 @@ extern "C" int edx_kron_spmm(const edx_kron* K, int k, const double* d_x, double
     cudaStream_t st = as_stream(stream);
     EDX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
     alignas(64) CUtensorMap tm;
-    if (!gather_of(K, variant) && (rc = kron_tensor_map(K, reinterpret_cast<const double2*>(d_x), k, 0, &tm)))
+    if (!gather_of(K, variant, k) && (rc = kron_tensor_map(K, reinterpret_cast<const double2*>(d_x), k, 0, &tm)))
         return rc;
     KrylovState S{};
     rc = launch_kron<false>(K, &tm, reinterpret_cast<const double2*>(d_x), reinterpret_cast<double2*>(d_y), S, k, 0,

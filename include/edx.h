@@ -229,8 +229,9 @@ typedef struct edx_kron {
  * slabs are staged in shared memory by the tensor-memory accelerator (2-D tiled loads of
  * 32-row boxes; no multicast); it needs slabs of at most 1024 rows whose ring of three
  * staged slabs fits in shared memory (about 590 rows: up to 11 bath orbitals).  GATHER: every
- * thread reads its row's source rows from global memory (any slab size).  AUTO: STAGED when
- * it fits, else GATHER. */
+ * thread reads its row's source rows from global memory (any slab size).  AUTO: GATHER for
+ * up to 8 columns or when STAGED does not fit, else STAGED (the faster of the two on wide
+ * blocks). */
 #define EDX_KRON_AUTO 0
 #define EDX_KRON_STAGED 1
 #define EDX_KRON_GATHER 2

@@ -48,7 +48,7 @@ def _rand(n, k, seed):
 
 @pytest.mark.parametrize("nbath,N,mode", [(4, 6, "ham_i"), (4, 5, "ham_n"), (6, 7, "ham_i"), (6, 7, "ham_n")])
 @pytest.mark.parametrize("k", [1, 2, 3, 6, 8, 13, 16, 40])
-@pytest.mark.parametrize("variant", [0, 2])  # automatic (staged here), gather
+@pytest.mark.parametrize("variant", [0, 1, 2])  # automatic, staged, gather
 def test_kron_spmm_equals_csr(cuda, nbath, N, mode, k, variant):
     from edrixs_b200 import device
     H, K = _both(nbath, N, mode)
@@ -89,7 +89,7 @@ def test_permute_rows_round_trip(cuda):
 
 
 @pytest.mark.parametrize("mode,k", [("ham_i", 6), ("ham_n", 6), ("ham_i", 40)])
-@pytest.mark.parametrize("variant", [0, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 def test_kron_lanczos_equals_csr(cuda, mode, k, variant):
     from edrixs_b200 import device
     H, K = _both(6, 7, mode)

@@ -643,17 +643,21 @@ def run_ours(args):
             # slab, source and bath tables
             tables = sum(x.numel() * x.element_size() for x in kron.t.values())
             per_launch = tables + 3 * k * rows * 16
+            model = "slab form: tables + 3 x k x rows x 16 B (V_cur read, V_prev read and written; no matrix stream)"
         elif packed is not None:
             # what the packed product must read once: entry words, row pointers, diagonal, table
             per_launch = (packed.ent.numel() * 4 + (rows + 1) * 8 + rows * 16 + packed.vals.numel() * 16
                           + 3 * k * rows * 16)
+            model = ("packed form: 4 B per entry word + 8 B per row pointer + 16 B diagonal per row + value "
+                     "table + 3 x k x rows x 16 B")
         else:
             per_launch = nnz * (sv + 4) + (rows + 1) * 8 + 3 * k * rows * 16
+            model = "CSR: (value + 4 B column) per entry + 8 B per row pointer + 3 x k x rows x 16 B"
         avg_ms = ms / max(launches, 1)
         ach = per_launch / (avg_ms / 1e3) / 1e9
         return dict(bound="hbm", achieved=round(ach, 1), peak=peak, unit="GB/s", frac=round(ach / peak, 4),
-                    traffic=None, bytes_per_launch=int(per_launch), avg_launch_us=round(avg_ms * 1e3, 2),
-                    launches=launches, total_ms=round(ms, 3))
+                    traffic=None, bytes_per_launch=int(per_launch), bytes_model=model,
+                    avg_launch_us=round(avg_ms * 1e3, 2), launches=launches, total_ms=round(ms, 3))
 
     r_hf = roof(st["hf_nnz"], st["hf_rows"], st["k_hf"], st["hf_apply_ms"], st["hf_iterations"], args.c64,
                 P.packed.get("hf") if st.get("hf_packed") else None, P.kron.get("hf") if st.get("hf_kron") else None)
